@@ -1,0 +1,198 @@
+/*
+ * ref_wrap.cu -- ORACLE TEST INFRASTRUCTURE.  Only tests/, the smoke check and the
+ * bench's CPU-baseline leg load the library built from this file; the product never does.
+ *
+ * This translation unit compiles the reference's canonical source, cudaSpmv.cu, UNCHANGED
+ * (the file is #included from where it lies; the build recipe passes its path as
+ * REF_CUDASPMV), renames its main() to ref_main(), and exposes C entry points around the
+ * reference's own host functions so that Python (ctypes) can call them:
+ *
+ *   ref_ncsr           -> ncsr               (cudaSpmv.cu:451-466, OpenMP CPU CSR SpMV)
+ *   ref_init_vec       -> init_vec           (cudaSpmv.cu:440-447, x[i] = i)
+ *   ref_get_errors     -> get_errors         (cudaSpmv.cu:474-495)
+ *   ref_stats          -> printMatrixStats   (cudaSpmv.cu:332-381, fills rl[], writes .sta)
+ *   ref_k1_*           -> getFormatDataK1    (cudaSpmv.cu:782-846)
+ *   ref_axc_*          -> getFormatDataAXC   (cudaSpmv.cu:1004-1062)
+ *   ref_axt_*          -> getFormatDataAXT   (cudaSpmv.cu:1391-1566)
+ *
+ * No reference code is copied here: the wrappers only marshal arguments into the
+ * reference's own structs (str_matCSR, str_matK1, str_matAXC, str_matAXT) and back out.
+ */
+#include <stdint.h>
+#define main ref_main
+#include REF_CUDASPMV
+#undef main
+
+namespace {
+
+struct RefCSR {
+    str_matCSR m;
+};
+
+/* Build a str_matCSR view of caller arrays; rl[] is the row length as the reference
+ * defines it (cudaSpmv.cu:339: rl = row[i+1] - row[i]). */
+static str_matCSR make_csr(UIN nrows, UIN nnz, const FPT *val, const UIN *col,
+                           const UIN *row, UIN *rl)
+{
+    str_matCSR m;
+    memset(&m, 0, sizeof(m));
+    strcpy(m.name, "oracle");
+    m.nrows = nrows;
+    m.nnz = nnz;
+    m.val = (FPT *)val;
+    m.col = (UIN *)col;
+    m.row = (UIN *)row;
+    m.rl = rl;
+    for (UIN i = 0; i < nrows; i++) rl[i] = row[i + 1] - row[i];
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_ncsr(UIN ompNT, UIN nrows, UIN nnz, const FPT *val, const UIN *col,
+              const UIN *row, const FPT *vec, FPT *res)
+{
+    UIN *rl = (UIN *)malloc((size_t)(nrows ? nrows : 1) * sizeof(UIN));
+    str_matCSR m = make_csr(nrows, nnz, val, col, row, rl);
+    ncsr(ompNT, m, vec, res);
+    free(rl);
+}
+
+void ref_init_vec(UIN ompNT, UIN len, FPT *vec) { init_vec(ompNT, len, vec); }
+
+void ref_get_errors(UIN len, const FPT *ar, const FPT *ac, double *aErr, double *rErr,
+                    UIN *pos)
+{
+    str_err e;
+    get_errors(len, ar, ac, &e);
+    *aErr = e.aErr;
+    *rErr = e.rErr;
+    *pos = e.pos;
+}
+
+/* printMatrixStats writes "<path up to the first '.'>.sta"; callers pass a scratch path. */
+void ref_stats(const char *path, UIN nrows, UIN nnz, const FPT *val, const UIN *col,
+               const UIN *row, UIN *rl_out, double *out5)
+{
+    str_matCSR m;
+    memset(&m, 0, sizeof(m));
+    m.nrows = nrows;
+    m.nnz = nnz;
+    m.val = (FPT *)val;
+    m.col = (UIN *)col;
+    m.row = (UIN *)row;
+    m.rl = rl_out;
+    printMatrixStats(path, &m);
+    out5[0] = m.rmin;
+    out5[1] = m.rave;
+    out5[2] = m.rmax;
+    out5[3] = m.rsd;
+    out5[4] = m.bw;
+}
+
+/* ---------------- K1 ---------------- */
+void *ref_k1(UIN nrows, UIN nnz, const FPT *val, const UIN *col, const UIN *row,
+             const FPT *vec, double *fd3)
+{
+    UIN *rl = (UIN *)malloc((size_t)(nrows ? nrows : 1) * sizeof(UIN));
+    str_matCSR m = make_csr(nrows, nnz, val, col, row, rl);
+    str_matK1 *k = (str_matK1 *)calloc(1, sizeof(str_matK1));
+    str_formatData fd = getFormatDataK1(CHUNK_SIZE, m, vec, k);
+    fd3[0] = fd.mfp;
+    fd3[1] = fd.beta;
+    fd3[2] = fd.ct;
+    free(rl);
+    return k;
+}
+void ref_k1_dims(void *h, UIN *d4)
+{
+    str_matK1 *k = (str_matK1 *)h;
+    d4[0] = k->nrows; d4[1] = k->nnz; d4[2] = k->chunkNum; d4[3] = k->lenVC;
+}
+void ref_k1_copy(void *h, UIN *permi, UIN *nmc, UIN *chp, FPT *val, UIN *col)
+{
+    str_matK1 *k = (str_matK1 *)h;
+    memcpy(permi, k->permi, (size_t)(k->chunkNum + 1) * CHUNK_SIZE * sizeof(UIN));
+    memcpy(nmc, k->nmc, (size_t)k->chunkNum * sizeof(UIN));
+    memcpy(chp, k->chp, (size_t)k->chunkNum * sizeof(UIN));
+    memcpy(val, k->val, (size_t)k->lenVC * sizeof(FPT));
+    memcpy(col, k->col, (size_t)k->lenVC * sizeof(UIN));
+}
+void ref_k1_free(void *h)
+{
+    str_matK1 *k = (str_matK1 *)h;
+    free(k->permi); free(k->nmc); free(k->chp); free(k->val); free(k->col); free(k);
+}
+
+/* ---------------- AXC ---------------- */
+void *ref_axc(UIN ompNT, UIN hbs, UIN nrows, UIN nnz, const FPT *val, const UIN *col,
+              const UIN *row, const FPT *vec, double *fd3)
+{
+    UIN *rl = (UIN *)malloc((size_t)(nrows ? nrows : 1) * sizeof(UIN));
+    str_matCSR m = make_csr(nrows, nnz, val, col, row, rl);
+    str_matAXC *a = (str_matAXC *)calloc(1, sizeof(str_matAXC));
+    str_formatData fd = getFormatDataAXC(ompNT, hbs, m, vec, a);
+    fd3[0] = fd.mfp;
+    fd3[1] = fd.beta;
+    fd3[2] = fd.ct;
+    free(rl);
+    return a;
+}
+void ref_axc_dims(void *h, UIN *d6)
+{
+    str_matAXC *a = (str_matAXC *)h;
+    d6[0] = a->nrows; d6[1] = a->nnz; d6[2] = a->hbs; d6[3] = a->lenAX; d6[4] = a->lenBRP;
+    d6[5] = a->lenMAPX;
+}
+void ref_axc_copy(void *h, FPT *ax, UIN *brp, UIN *mapx)
+{
+    str_matAXC *a = (str_matAXC *)h;
+    memcpy(ax, a->ax, (size_t)a->lenAX * sizeof(FPT));
+    memcpy(brp, a->brp, (size_t)a->lenBRP * sizeof(UIN));
+    memcpy(mapx, a->mapx, (size_t)a->lenMAPX * sizeof(UIN));
+}
+void ref_axc_free(void *h)
+{
+    str_matAXC *a = (str_matAXC *)h;
+    free(a->ax); free(a->brp); free(a->mapx); free(a);
+}
+
+/* ---------------- AXT ---------------- */
+void *ref_axt(UIN ompNT, UIN bs, UIN thw, UIN th, const char *mode, UIN nrows, UIN nnz,
+              const FPT *val, const UIN *col, const UIN *row, const FPT *vec, double *fd3,
+              char *name48)
+{
+    UIN *rl = (UIN *)malloc((size_t)(nrows ? nrows : 1) * sizeof(UIN));
+    str_matCSR m = make_csr(nrows, nnz, val, col, row, rl);
+    str_matAXT *a = (str_matAXT *)calloc(1, sizeof(str_matAXT));
+    str_formatData fd = getFormatDataAXT(ompNT, bs, thw, th, mode, m, vec, a);
+    fd3[0] = fd.mfp;
+    fd3[1] = fd.beta;
+    fd3[2] = fd.ct;
+    if (name48) memcpy(name48, fd.name, 48);
+    free(rl);
+    return a;
+}
+void ref_axt_dims(void *h, UIN *d11)
+{
+    str_matAXT *a = (str_matAXT *)h;
+    d11[0] = a->nrows; d11[1] = a->nnz; d11[2] = a->tileHW; d11[3] = a->tileH;
+    d11[4] = a->logTH; d11[5] = a->tileN; d11[6] = a->lenAX; d11[7] = a->lenSEC;
+    d11[8] = a->lenCON; d11[9] = a->log; d11[10] = a->bs;
+}
+void ref_axt_copy(void *h, FPT *ax, UIN *sec, UIN *con)
+{
+    str_matAXT *a = (str_matAXT *)h;
+    memcpy(ax, a->ax, (size_t)a->lenAX * sizeof(FPT));
+    memcpy(sec, a->sec, (size_t)a->lenSEC * sizeof(UIN));
+    memcpy(con, a->con, (size_t)(a->lenCON + 1) * sizeof(UIN));
+}
+void ref_axt_free(void *h)
+{
+    str_matAXT *a = (str_matAXT *)h;
+    free(a->ax); free(a->sec); free(a->con); free(a);
+}
+
+}  // extern "C"
