@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""SpMV benchmark of the B200 engine (one JSON line on stdout, rank 0).
+
+Default workload: FP64 AXT SpMV (the engine's native AXT layout, x gathered at SpMV time)
+on the power-law matrix -- 4,194,304 rows, 67,108,864 nnz, lognormal(2.5, 1.2) row
+lengths clipped to [1, 10000] and rescaled, columns uniform without replacement, values
+N(0,1), x uniform[-1,1], seed 1.  A step is one SpMV of the whole matrix (one kernel
+launch).  The value/column streams (805 MB) are larger than the 126 MB L2, so no L2 flush
+is inserted between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--workload powerlaw|laplacian|stencil27|powerlaw-small]
+                  [--variant axt-com-th1|axt-unc-th1-hw4|csr|k1|axc|...] [--sweep]
+
+Under torchrun (N > 1) every rank owns an independent partition of the same size (its own
+power-law block, seed 1 + rank: a block-diagonal operator, no exchange on the data path),
+so per-GPU work is fixed ("weak" scaling); the time is the max over ranks.
+``--impl reference`` times the reference's own CPU CSR SpMV (ncsr, cudaSpmv.cu:451,
+compiled unchanged into oracle/_ref) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV GFLOP/s & HBM GB/s (% of 8 TB/s), FP64 vs mixed/batched/adjoint, 1 B200"
+
+WORKLOADS = {
+    "powerlaw": dict(desc="power-law 4194304 rows x 67108864 nnz, lognormal(2.5,1.2) "
+                          "lengths clipped [1,10000], FP64, x U[-1,1]",
+                     seed=1, xseed=1),
+    "powerlaw-small": dict(desc="power-law 1048576 rows x 16777216 nnz (profiling case), "
+                                "FP64", seed=1, xseed=1),
+    "laplacian": dict(desc="2D 5-point Laplacian 512x512 (262144 rows, 1308672 nnz), FP64, "
+                           "x U[-1,1]", seed=0, xseed=0),
+    "stencil27": dict(desc="3D 27-point stencil 160^3 (4096000 rows, 109215352 nnz), FP64, "
+                           "x N(0,1)", seed=2, xseed=2),
+}
+
+VARIANTS = {
+    "csr": dict(fmt="CSR"),
+    "k1": dict(fmt="K1"),
+    "axc": dict(fmt="AXC", hbs=32),
+    "axt-com-th1": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256),
+    "axt-com-th4": dict(fmt="AXT", mode="COM", tileH=4, tileHW=32, bs=256),
+    "axt-com-th8": dict(fmt="AXT", mode="COM", tileH=8, tileHW=32, bs=256),
+    "axt-unc-th1-hw4": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
+    "axt-unc-th1-hw8": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=8),
+    "axt-unc-th1-hw16": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=16),
+    "axt-unc-th2": dict(fmt="AXT", mode="UNC", tileH=2, tileHW=32),
+    "axt-unc-th4": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
+    "axt-unc-th8": dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
+}
+DEFAULT_VARIANT = "axt-com-th1"
+
+
+def make_matrix(workload: str, rank: int):
+    from gpu_spmv_b200 import matgen
+
+    w = WORKLOADS[workload]
+    if workload == "powerlaw":
+        row, col, val = matgen.powerlaw(seed=w["seed"] + rank)
+        x = matgen.vector(len(row) - 1, "uniform", -1.0, 1.0, seed=w["xseed"] + 1000 + rank)
+    elif workload == "powerlaw-small":
+        row, col, val = matgen.powerlaw(nrows=1048576, nnz=16777216, seed=w["seed"] + rank)
+        x = matgen.vector(len(row) - 1, "uniform", -1.0, 1.0, seed=w["xseed"] + 1000 + rank)
+    elif workload == "laplacian":
+        row, col, val = matgen.laplacian2d(512)
+        x = matgen.vector(len(row) - 1, "uniform", -1.0, 1.0, seed=w["xseed"] + rank)
+    elif workload == "stencil27":
+        row, col, val = matgen.stencil27(160, seed=w["seed"] + rank)
+        x = matgen.vector(len(row) - 1, "normal", seed=w["xseed"] + rank)
+    else:
+        raise KeyError(workload)
+    return row, col, val, x
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_lookup(key: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(p)).get(key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.lines: list[str] = []
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            ident = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", ident], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [s.strip() for s in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_spmv(row, col, val, x, budget_s=15.0, threads=None):
+    """The reference's ncsr (OpenMP) on the host cores; returns (GFLOP/s, sample text)."""
+    from oracle.oracle import Ref
+
+    R = Ref()
+    threads = threads or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    R.ncsr(row, col, val, x, threads=threads)  # warm-up (page-in)
+    t1 = time.perf_counter()
+    reps = max(1, min(50, int(budget_s / max(t1 - t0, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        R.ncsr(row, col, val, x, threads=threads)
+    dt = (time.perf_counter() - t0) / reps
+    nnz = len(col)
+    return 2.0 * nnz / dt / 1e9, f"{reps} full SpMVs of the workload ({nnz} nnz)", threads
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    try:
+        from oracle.oracle import Ref
+
+        if not Ref.available():
+            raise FileNotFoundError("oracle/_ref not built")
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build missing: {e}"}))
+        return 0
+    row, col, val, x = make_matrix(args.workload, 0)
+    from oracle.oracle import Ref
+
+    R = Ref()
+    threads = os.cpu_count() or 1
+    n, nnz = len(row) - 1, len(col)
+    # each step is a bounded sample: a rotating block of rows sized so that the whole run
+    # stays within ~2 minutes
+    t0 = time.perf_counter()
+    R.ncsr(row, col, val, x, threads=threads)
+    t_full = time.perf_counter() - t0
+    total_steps = args.steps + args.warmup
+    frac = min(1.0, 120.0 / max(total_steps * t_full, 1e-9))
+    nb = max(1, int(round(1.0 / frac)))
+    blocks = np.linspace(0, n, nb + 1).astype(np.int64)
+    subs = []
+    for b in range(nb):
+        r0, r1 = blocks[b], blocks[b + 1]
+        rr = (row[r0:r1 + 1] - row[r0]).astype(np.uint32)
+        subs.append((rr, col[row[r0]:row[r1]], val[row[r0]:row[r1]]))
+    for s in range(args.warmup):
+        rr, cc, vv = subs[s % nb]
+        R.ncsr(rr, cc, vv, x, threads=threads)
+    done_nnz, t = 0, 0.0
+    for s in range(args.steps):
+        rr, cc, vv = subs[s % nb]
+        t0 = time.perf_counter()
+        R.ncsr(rr, cc, vv, x, threads=threads)
+        t += time.perf_counter() - t0
+        done_nnz += len(cc)
+    value = 2.0 * done_nnz / t / 1e9
+    sample = (f"each step: one of {nb} row blocks (~{nnz // nb} nnz) of the workload, "
+              f"full SpMV takes {t_full:.3f} s on {threads} threads")
+    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOADS[args.workload]["desc"],
+                       "path": "reference ncsr (cudaSpmv.cu:451-466, OpenMP, compiled "
+                               "unchanged)", "threads": threads},
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import engine as E
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    row, col, val, x = make_matrix(args.workload, rank)
+    n, nnz = len(row) - 1, len(col)
+    variants = list(VARIANTS) if args.sweep else [args.variant]
+    results = {}
+    for vname in variants:
+        A = E.Matrix(row, col, val, ncols=n, **VARIANTS[vname])
+        dx = torch.from_numpy(x).cuda()
+        dy = torch.empty(n, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream()
+        for _ in range(args.warmup):
+            A.spmv(dx, dy)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        K = args.steps
+        sampler = ClockSampler(local) if (rank == 0 and not args.sweep) else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eb = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ea = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(K):
+            eb[k].record(stream)
+            A.spmv(dx, dy)
+            ea[k].record(stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.stop()
+        elapsed = ev0.elapsed_time(ev1)  # ms
+        kern = sum(b.elapsed_time(a) for b, a in zip(eb, ea)) / K
+        if dist:
+            t = torch.tensor([elapsed, kern], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            elapsed, kern = float(t[0]), float(t[1])
+        results[vname] = (A, elapsed, kern, sampler, dx, dy)
+        if args.sweep and rank == 0:
+            gf = 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
+            B = E.algorithmic_bytes(n, n, nnz)
+            print(f"[sweep] {vname:18s} {elapsed / K * 1e3:9.1f} us/step  {gf:8.1f} GFLOP/s  "
+                  f"{B / (kern * 1e-3) / 1e9:8.1f} GB/s alg  beta={A.info.beta:.3f} "
+                  f"conv={A.info.conv_ms:.1f} ms", file=sys.stderr, flush=True)
+        if args.sweep:
+            A.close()
+    if args.sweep:
+        return 0
+    A, elapsed, kern, sampler, dx, dy = results[args.variant]
+    K = args.steps
+    value = world * 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
+    B = E.algorithmic_bytes(n, n, nnz)
+    peak, peak_kind = measured_peak()
+    achieved = B / (kern * 1e-3) / 1e9
+    tkey = f"{args.workload}/{args.variant}"
+    traffic = traffic_lookup(tkey)
+
+    # ---- end to end through the C ABI with host buffers: H2D x, SpMV, D2H y per step
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.from_numpy(x).pin_memory()
+        hy = torch.empty(n, dtype=torch.float64).pin_memory()
+        Ke = min(K, args.e2e_steps)
+        lib = L.lib()
+        sh = E.stream_handle()
+        for _ in range(3):
+            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
+                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, 0, sh), "e2e")
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(Ke):
+            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
+                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, 0, sh), "e2e")
+        te = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([te], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t[0])
+        e2e = {"value": world * 2.0 * nnz * Ke / te / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n, "steps": Ke,
+               "path": "gs_spmv_host (C ABI): pinned host x -> device, SpMV, y -> host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, sample, threads = cpu_reference_spmv(row, col, val, x)
+            cpu = {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                   "sample": sample + "; reference ncsr compiled unchanged (oracle/_ref)"}
+        except Exception as e:  # the checker library is absent: report it
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    clocks = sampler.summary() if sampler else None
+    info = A.info
+    line = {
+        "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": elapsed / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload]["desc"],
+                   "format": args.variant, "nrows": n, "nnz": nnz, "beta": info.beta,
+                   "l2": "value/column streams > 126 MB L2 each step; no flush",
+                   "per_rank": "independent partition of the same size (block-diagonal)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "frac_of_8TBs": achieved / 8000.0, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": B, "kernel_ms": kern},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": K,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="powerlaw", choices=list(WORKLOADS))
+    ap.add_argument("--variant", default=DEFAULT_VARIANT, choices=list(VARIANTS))
+    ap.add_argument("--sweep", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,213 @@
+// gs_capi.cu -- the native C ABI (gs_*): matrix handles, SpMV dispatch, status strings.
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "gs_internal.cuh"
+
+namespace gs {
+const char *last_error_text();
+}
+
+namespace {
+UIN g_num_ite = 250;  // cudaSpmv.cu:96-98
+}
+
+extern "C" {
+
+const char *gs_status_string(gs_status s)
+{
+    switch (s) {
+    case GS_OK: return "GS_OK";
+    case GS_ERR_INVALID: return "GS_ERR_INVALID";
+    case GS_ERR_CUDA: return "GS_ERR_CUDA";
+    case GS_ERR_ALLOC: return "GS_ERR_ALLOC";
+    case GS_ERR_OVERFLOW: return "GS_ERR_OVERFLOW";
+    case GS_ERR_UNSUPPORTED: return "GS_ERR_UNSUPPORTED";
+    case GS_ERR_DEVICE: return "GS_ERR_DEVICE";
+    default: return "GS_ERR_UNKNOWN";
+    }
+}
+
+const char *gs_last_error(void) { return gs::last_error_text(); }
+
+const char *gs_version(void) { return "gpuspmv_b200 1.0 (sm_100a)"; }
+
+void gs_set_num_ite(UIN n) { g_num_ite = n ? n : 1; }
+UIN gs_get_num_ite(void) { return g_num_ite; }
+
+double gs_algorithmic_bytes(UIN nrows, UIN ncols, UIN nnz, UIN k, UIN s_v, UIN s_i, UIN s_x,
+                            UIN s_y)
+{
+    return (double)nnz * (s_v + s_i) + 4.0 * ((double)nrows + 1) + (double)s_x * ncols * k +
+           (double)s_y * nrows * k;
+}
+
+gs_status gs_matrix_create(gs_matrix **out, const gs_convert_params *params, UIN nrows,
+                           UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
+                           const void *d_val, gs_dtype val_type, gs_stream stream)
+{
+    gs::clear_error();
+    if (!out || !params) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    gs_matrix *A = new (std::nothrow) gs_matrix();
+    if (!A) return gs::fail(GS_ERR_ALLOC, "host allocation failed");
+    gs_status st = gs::convert(A, *params, nrows, ncols, nnz, d_row, d_col, d_val, val_type,
+                               nullptr, nullptr, gs::cs(stream));
+    if (st != GS_OK) {
+        cudaStreamSynchronize(gs::cs(stream));
+        delete A;
+        return st;
+    }
+    *out = A;
+    return GS_OK;
+}
+
+gs_status gs_matrix_destroy(gs_matrix *A)
+{
+    if (A) {
+        cudaDeviceSynchronize();  // no kernel may still read the buffers
+        delete A;
+    }
+    return GS_OK;
+}
+
+gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *i)
+{
+    if (!A || !i) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    memset(i, 0, sizeof(*i));
+    i->format = A->p.format;
+    i->nrows = A->nrows;
+    i->ncols = A->ncols;
+    i->nnz = A->nnz;
+    i->tileHW = A->tileHW;
+    i->tileH = A->tileH;
+    i->logTH = A->logTH;
+    i->tileN = A->tileN;
+    i->lenAX = A->lenAX;
+    i->lenSEC = A->lenSEC;
+    i->lenCON = A->lenCON;
+    i->log = A->log;
+    i->bs = A->bs;
+    i->mode = A->p.mode;
+    i->hbs = A->hbs;
+    i->lenBRP = A->lenBRP;
+    i->lenMAPX = A->lenMAPX;
+    i->chunkNum = A->chunkNum;
+    i->lenVC = A->lenVC;
+    i->nslots = A->nslots;
+    i->vtype = A->p.vtype;
+    i->itype = A->p.itype;
+    i->d_val = A->val.p;
+    i->d_col = A->col.p;
+    i->d_colbase = A->colbase.as<UIN>();
+    i->d_sec = A->sec.as<UIN>();
+    i->d_con = A->con.as<UIN>();
+    i->d_brp = A->brp.as<UIN>();
+    i->d_mapx = A->mapx.as<UIN>();
+    i->d_permi = A->permi.as<UIN>();
+    i->d_nmc = A->nmc.as<UIN>();
+    i->d_chp = A->chp.as<UIN>();
+    i->d_rpos = A->rpos.as<UIN>();
+    i->d_rlen = A->rlen.as<UIN>();
+    i->conv_ms = A->conv_ms;
+    i->mfp = A->mfp;
+    i->beta = A->beta;
+    return GS_OK;
+}
+
+gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y,
+                  gs_dtype ytype, UIN flags, gs_stream stream)
+{
+    if (!A || !d_x || !d_y) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    cudaStream_t s = gs::cs(stream);
+    if (A->p.format == GS_FMT_K1) {
+        if (xtype != GS_F64 || ytype != GS_F64)
+            return gs::fail(GS_ERR_UNSUPPORTED, "K1 takes FP64 x and y");
+        gs::K1Args a{};
+        a.nrows = A->nrows;
+        a.chunkNum = A->chunkNum;
+        a.permi = A->permi.as<uint32_t>();
+        a.nmc = A->nmc.as<uint32_t>();
+        a.chp = A->chp.as<uint32_t>();
+        a.klen = A->k1len.as<uint32_t>();
+        a.val = A->val.as<double>();
+        a.col = A->col.as<uint32_t>();
+        a.x = static_cast<const double *>(d_x);
+        a.y = static_cast<double *>(d_y);
+        a.unit_chunk = A->k1unit_chunk.as<uint32_t>();
+        a.unit_base = A->k1unit_base.as<uint32_t>();
+        a.units = A->k1units;
+        a.partial = A->k1partial.as<double>();
+        a.count = A->k1count.as<uint32_t>();
+        return gs::launch_k1(a, s);
+    }
+    const bool f64 = A->p.vtype == GS_F64;
+    if (f64 && xtype != GS_F64) return gs::fail(GS_ERR_UNSUPPORTED, "FP64 matrices take FP64 x");
+    if (!f64 && xtype != GS_F32)
+        return gs::fail(GS_ERR_UNSUPPORTED, "FP32/BF16 matrices take FP32 x");
+    gs::RowsArgs a{};
+    a.nrows = A->nrows;
+    a.rpos = A->rpos.as<uint32_t>();
+    a.rlen = A->rlen.as<uint32_t>();
+    a.val = A->val.p;
+    a.col = A->col.p;
+    a.colbase = A->colbase.as<uint32_t>();
+    a.x = d_x;
+    a.y = d_y;
+    a.thw = A->tileHW ? A->tileHW : 1;
+    a.th = A->tileH ? A->tileH : 1;
+    a.nslots = A->nslots;
+    return gs::launch_rows(a, A->p.vtype, A->p.itype, ytype, flags, A->tiled != 0, false,
+                           A->lane_pos, A->rpu, s);
+}
+
+gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dtype xtype,
+                       void *h_y, void *d_ybuf, gs_dtype ytype, UIN flags, gs_stream stream)
+{
+    if (!A || !h_x || !h_y || !d_xbuf || !d_ybuf)
+        return gs::fail(GS_ERR_INVALID, "NULL argument");
+    cudaStream_t s = gs::cs(stream);
+    GS_CUDA(cudaMemcpyAsync(d_xbuf, h_x, (size_t)A->ncols * gs::dtype_size(xtype),
+                            cudaMemcpyHostToDevice, s));
+    GS_TRY(gs_spmv(A, d_xbuf, xtype, d_ybuf, ytype, flags, stream));
+    GS_CUDA(cudaMemcpyAsync(h_y, d_ybuf, (size_t)A->nrows * gs::dtype_size(ytype),
+                            cudaMemcpyDeviceToHost, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    return GS_OK;
+}
+
+gs_status gs_copy_to_host(void *h_dst, const void *d_src, size_t bytes)
+{
+    if (!bytes) return GS_OK;
+    if (!h_dst || !d_src) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    GS_CUDA(cudaMemcpy(h_dst, d_src, bytes, cudaMemcpyDeviceToHost));
+    return GS_OK;
+}
+
+gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
+                          const double *d_val, const double *d_x, double *d_y,
+                          gs_stream stream)
+{
+    (void)ncols;
+    if (nrows == 0) return GS_OK;
+    if (!d_row || !d_x || !d_y || (nnz && (!d_col || !d_val)))
+        return gs::fail(GS_ERR_INVALID, "NULL argument");
+    if ((reinterpret_cast<uintptr_t>(d_val) & 15u) || (reinterpret_cast<uintptr_t>(d_col) & 15u))
+        return gs::fail(GS_ERR_INVALID, "val and col must be 16-byte aligned");
+    gs::RowsArgs a{};
+    a.nrows = nrows;
+    a.rpos = d_row;
+    a.rlen = nullptr;
+    a.val = d_val;
+    a.col = d_col;
+    a.x = d_x;
+    a.y = d_y;
+    a.thw = 1;
+    a.th = 1;
+    a.nslots = nnz;
+    return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, false, false, 4,
+                           gs::choose_rpu(nrows, nnz, 4), gs::cs(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+// gs_internal.cuh -- internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstddef>
+
+#include "gpuspmv_b200.h"
+
+namespace gs {
+
+// ------------------------------------------------------------------ errors
+// Records a formatted message for gs_last_error() on the calling thread and returns st.
+gs_status fail(gs_status st, const char *fmt, ...);
+void clear_error();
+
+#define GS_CUDA(call)                                                                    \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return ::gs::fail(GS_ERR_CUDA, "%s:%d: %s failed: %s", __FILE__, __LINE__,  \
+                              #call, cudaGetErrorString(e_));                            \
+    } while (0)
+
+#define GS_TRY(call)                                                                     \
+    do {                                                                                 \
+        gs_status s_ = (call);                                                           \
+        if (s_ != GS_OK) return s_;                                                      \
+    } while (0)
+
+#define GS_CHECK_LAUNCH() GS_CUDA(cudaGetLastError())
+
+inline cudaStream_t cs(gs_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline size_t dtype_size(gs_dtype t) { return t == GS_F64 ? 8 : (t == GS_F32 ? 4 : 2); }
+
+// ------------------------------------------------------------------ device buffers
+// Owning device allocation (cudaMalloc / cudaFree).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) { reset(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { reset(); }
+    void reset() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    gs_status alloc(size_t nbytes);                       // rounds up, keeps 16 B of tail slack
+    gs_status alloc_zero(size_t nbytes, cudaStream_t s);  // alloc + async memset 0
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ------------------------------------------------------------------ scan primitives
+// Exclusive prefix sum of n 32-bit counts produced by `count(i)`, written as 64-bit
+// offsets out[0..n] (out[n] = total).  Implemented in gs_scan.cu for the functors listed
+// there; `total` receives out[n] on the host (synchronises the stream).
+enum class CountKind {
+    RowLen,         // row[i+1]-row[i]
+    RowTiles,       // ceil((row[i+1]-row[i]) / a)
+    Array,          // arr[i]
+    ArrayTimes,     // arr[i] * a
+    BitZero,        // (arr[i] >> a) & 1 == 0   (radix sort pass)
+    PiecesMin1,     // max(1, ceil(arr[i] / a))
+};
+struct CountSpec {
+    CountKind kind;
+    const uint32_t *row = nullptr;  // RowLen / RowTiles
+    const uint32_t *arr = nullptr;  // Array / ArrayTimes
+    uint32_t a = 1;
+};
+gs_status exclusive_scan(const CountSpec &spec, size_t n, uint64_t *out, uint64_t *total,
+                         cudaStream_t s);
+
+// Stable sort of row indices 0..n-1 by descending key (keys < 2^bits): idx_out[i] is the
+// i-th row.  Ties keep ascending row order.  1-bit LSD radix passes built on the scan.
+gs_status stable_sort_desc(const uint32_t *key, uint32_t n, uint32_t max_key,
+                           uint32_t *idx_out, cudaStream_t s);
+
+// Maximum of n u32 values (host result, synchronises).
+gs_status reduce_max_u32(const uint32_t *d, size_t n, uint32_t *out, cudaStream_t s);
+
+// ------------------------------------------------------------------ device helpers
+__device__ __forceinline__ double ldcs_f64(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ uint32_t ldcs_u32(const uint32_t *p) { return __ldcs(p); }
+
+template <class T> struct ValTraits;
+template <> struct ValTraits<double> {
+    __device__ __forceinline__ static double to_f64(double v) { return v; }
+    __device__ __forceinline__ static float to_f32(double v) { return (float)v; }
+};
+template <> struct ValTraits<float> {
+    __device__ __forceinline__ static double to_f64(float v) { return (double)v; }
+    __device__ __forceinline__ static float to_f32(float v) { return v; }
+};
+template <> struct ValTraits<__nv_bfloat16> {
+    __device__ __forceinline__ static double to_f64(__nv_bfloat16 v) {
+        return (double)__bfloat162float(v);
+    }
+    __device__ __forceinline__ static float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
+
+}  // namespace gs
+
+// ------------------------------------------------------------------ the matrix handle
+struct gs_matrix {
+    gs_convert_params p{};
+    uint32_t nrows = 0, ncols = 0, nnz = 0;
+    // reference-layout dimensions
+    uint32_t tileHW = 0, tileH = 0, logTH = 0, tileN = 0, lenAX = 0, lenSEC = 0, lenCON = 0,
+             log = 0, bs = 0;
+    uint32_t hbs = 0, lenBRP = 0, lenMAPX = 0;
+    uint32_t chunkNum = 0, lenVC = 0;
+    // native streams
+    uint32_t nslots = 0;
+    gs::DevBuf val, col, colbase;
+    gs::DevBuf sec, con, brp, mapx;
+    gs::DevBuf permi, nmc, chp;
+    gs::DevBuf rpos, rlen;  // row table for the row-stream kernels
+    // K1 execution plan (split of long chunks) and its scratch
+    gs::DevBuf k1len, k1unit_chunk, k1unit_base, k1partial, k1count;
+    uint32_t k1units = 0;
+    // row-stream kernel configuration
+    uint32_t tiled = 0;    // 1: positions map to tile slots (tileH > 1 layouts)
+    uint32_t lane_pos = 4; // positions per lane per window
+    uint32_t rpu = 32;     // rows per warp unit
+    double conv_ms = 0, mfp = 0, beta = 0;
+};
+
+namespace gs {
+
+// Row-stream SpMV over a position table (see gs_spmv_rows.cu).
+struct RowsArgs {
+    uint32_t nrows;
+    const uint32_t *rpos;   // nrows+1 first positions
+    const uint32_t *rlen;   // real lengths or nullptr (rows unpadded)
+    const void *val;        // value stream (or baked ax)
+    const void *col;        // column stream (u32 or u16 offsets)
+    const uint32_t *colbase;// per-unit base for u16 offsets
+    const void *x;
+    void *y;
+    uint32_t thw, th;       // tile shape for tiled position->slot mapping
+    uint32_t axw;           // baked: ax half width (tileHW or hbs)
+    uint32_t nslots;        // length of the value/column streams (vector loads stop short)
+};
+gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
+                      uint32_t flags, bool tiled, bool baked, uint32_t lane_pos, uint32_t rpu,
+                      cudaStream_t s);
+uint32_t choose_rpu(uint32_t nrows, uint64_t positions, uint32_t lane_pos);
+
+// K1 SpMV (see gs_spmv_k1.cu).
+struct K1Args {
+    uint32_t nrows, chunkNum;
+    const uint32_t *permi, *nmc, *chp, *klen;  // klen: per sorted row length or nullptr
+    const double *val;
+    const uint32_t *col;
+    const double *x;
+    double *y;
+    const uint32_t *unit_chunk, *unit_base;  // plan
+    uint32_t units;
+    double *partial;
+    uint32_t *count;
+};
+gs_status launch_k1(const K1Args &a, cudaStream_t s);
+// Build the K1 plan for chunk lengths nmc (device) into the given buffers.
+constexpr uint32_t kK1Split = 256;  // j-steps per K1 work unit
+gs_status build_k1_plan(const uint32_t *d_nmc, uint32_t chunkNum, DevBuf &unit_chunk,
+                        DevBuf &unit_base, DevBuf &partial, DevBuf &count, uint32_t *units,
+                        cudaStream_t s);
+
+// Conversion entry (gs_convert.cu).  x/ax optional: bake x into a reference-layout ax.
+gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t nrows, uint32_t ncols,
+                  uint32_t nnz, const uint32_t *d_row, const uint32_t *d_col,
+                  const void *d_val, gs_dtype val_type, const double *d_xbake,
+                  DevBuf *ax_out, cudaStream_t s);
+
+}  // namespace gs

@@ -1,0 +1,682 @@
+// gs_refapi.cu -- the drop-in layer: the reference program's host API (cudaSpmv.cu) with
+// the same names, struct layouts and argument meaning, backed by the engine.
+//
+// Differences from the reference, all deliberate:
+//  * converters run on the GPU (device scans / sort / scatter) and return the same host
+//    arrays bit for bit; fd.ct is the device conversion time;
+//  * entry points never exit(): failures print a message, return a result named "error"
+//    (times 0) and leave the reason in gs_last_error();
+//  * AXT entry points accept any tileHW (the reference's kernels hard-code 16/8/4/32) and
+//    take the launch shape (wpw, tpw, cudaBlockSize) only for the result name;
+//  * the AXT/AXC kernels write every y entry once, so y needs no memset between launches
+//    (the reference memsets it outside its timing window, cudaSpmv.cu:1631);
+//  * COM headers are decoded so that a header word equal to 0 (row 0, offset 0) still
+//    counts -- gaxtch1 drops it (cudaSpmv.cu:2089).
+#include <cusparse.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+
+#include "gs_internal.cuh"
+
+extern "C" UIN gs_get_num_ite(void);
+
+namespace {
+
+using gs::DevBuf;
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer() { cudaEventCreate(&a); cudaEventCreate(&b); }
+    ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+};
+
+str_res error_res(const char *name, const char *what)
+{
+    str_res r;
+    memset(&r, 0, sizeof(r));
+    strcpy(r.name, "error");
+    fflush(stdout);
+    printf("%s: %s\n", name, what);
+    fflush(stdout);
+    return r;
+}
+
+str_formatData error_fd(const char *name)
+{
+    str_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    strcpy(fd.name, "error");
+    fflush(stdout);
+    printf("%s: %s\n", name, gs_last_error());
+    fflush(stdout);
+    return fd;
+}
+
+template <class T> gs_status h2d(DevBuf &b, const T *h, size_t n)
+{
+    GS_TRY(b.alloc(n * sizeof(T)));
+    if (n) GS_CUDA(cudaMemcpy(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return GS_OK;
+}
+
+template <class T> T *d2h_calloc(const void *d, size_t n)
+{
+    T *h = static_cast<T *>(calloc(n ? n : 1, sizeof(T)));
+    if (h && n) cudaMemcpy(h, d, n * sizeof(T), cudaMemcpyDeviceToHost);
+    return h;
+}
+
+// Times gs_get_num_ite() launches of `launch` (legacy default stream, CUDA events around
+// each launch, as the reference's test_* loops do), then scores y against ref.
+str_res timed(const char *name, UIN nrows, UIN nnz, const std::function<gs_status()> &launch,
+              const DevBuf &dy, const FPT *ref)
+{
+    const UIN ite = gs_get_num_ite();
+    Timer t;
+    float tt = 0.f;
+    for (UIN i = 0; i < ite; i++) {
+        cudaEventRecord(t.a, 0);
+        gs_status st = launch();
+        cudaEventRecord(t.b, 0);
+        cudaEventSynchronize(t.b);
+        if (st != GS_OK) return error_res(name, gs_last_error());
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        tt += ms;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return error_res(name, cudaGetErrorString(e));
+    str_res sr;
+    memset(&sr, 0, sizeof(sr));
+    snprintf(sr.name, sizeof(sr.name), "%s", name);
+    sr.et = ((double)tt / (double)ite) * 1e-3;
+    sr.ot = 0.0;
+    sr.flops = (2.0 * (double)nnz) / sr.et;
+    FPT *res = d2h_calloc<FPT>(dy.p, nrows);
+    get_errors(nrows, ref, res, &sr.sErr);
+    free(res);
+    return sr;
+}
+
+// rpos[r] = src[r] / div  (UNC tileH=1 con, AXC brp -> first slot of each row)
+__global__ void k_div_table(uint32_t n1, const uint32_t *src, uint32_t div, uint32_t *rpos)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n1) rpos[i] = src[i] / div;
+}
+
+// UNC tileH>1: rpos[r] = th * (first tile column of r), from con[r] = t*2*ths + c;
+// rpos[n] = tileN * th * thw (trailing unused columns count as padding of the last row).
+__global__ void k_unc_table(uint32_t n, const uint32_t *con, uint32_t thw, uint32_t th,
+                            uint32_t tileN, uint32_t *rpos)
+{
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ths = thw * th;
+    if (r < n) rpos[r] = th * ((con[r] / (2 * ths)) * thw + con[r] % thw);
+    if (r == n) rpos[n] = tileN * ths;
+}
+
+// COM: recover row lengths from the header words.  Position p (CSR order) is a segment
+// start iff it opens a segment block (p % blk == 0, blk = bs for tileH=1, th for tileH>1:
+// the reference always writes a header there) or its header word is non-zero; the
+// segment covers offset+1 positions of row hdr >> log.
+__global__ void k_com_rowlen(uint32_t nnz, uint32_t n, const uint32_t *sec, uint32_t thw,
+                             uint32_t th, uint32_t blk, uint32_t log, uint32_t *rl,
+                             uint32_t *flag)
+{
+    const uint32_t ths = thw * th;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz;
+         p += gridDim.x * blockDim.x) {
+        uint32_t slot = p;
+        if (th > 1) {
+            const uint32_t t = p / ths, rem = p - t * ths, c = rem / th;
+            slot = t * ths + (rem - c * th) * thw + c;
+        }
+        const uint32_t h = sec[slot];
+        if (p % blk == 0 || h != 0) {
+            const uint32_t r = h >> log, o = h & (blk - 1);
+            if (r >= n) { atomicOr(flag, 1u); continue; }
+            atomicAdd(rl + r, o + 1);
+        }
+    }
+}
+
+__global__ void k_narrow(uint32_t n1, const uint64_t *a, uint32_t *b)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n1) b[i] = (uint32_t)a[i];
+}
+
+gs_status com_rpos(const str_matAXT &m, const DevBuf &dsec, DevBuf &rpos)
+{
+    const uint32_t blk = m.tileH == 1 ? m.bs : m.tileH;
+    if (blk == 0 || (blk & (blk - 1)) != 0 || (1u << m.log) != blk)
+        return gs::fail(GS_ERR_UNSUPPORTED,
+                        "COM headers decode only for a power-of-two %s (got %u, log %u)",
+                        m.tileH == 1 ? "bs" : "tileH", blk, m.log);
+    DevBuf rl, flag, P;
+    GS_TRY(rl.alloc_zero((size_t)m.nrows * 4 + 4, 0));
+    GS_TRY(flag.alloc_zero(4, 0));
+    k_com_rowlen<<<1184, 256>>>(m.nnz, m.nrows, dsec.as<uint32_t>(), m.tileHW, m.tileH, blk,
+                                m.log, rl.as<uint32_t>(), flag.as<uint32_t>());
+    GS_CHECK_LAUNCH();
+    uint32_t hf = 0;
+    GS_CUDA(cudaMemcpy(&hf, flag.p, 4, cudaMemcpyDeviceToHost));
+    if (hf) return gs::fail(GS_ERR_INVALID, "COM header names a row beyond nrows");
+    GS_TRY(P.alloc(((size_t)m.nrows + 1) * 8));
+    gs::CountSpec cs{gs::CountKind::Array};
+    cs.arr = rl.as<uint32_t>();
+    uint64_t total = 0;
+    GS_TRY(gs::exclusive_scan(cs, m.nrows, P.as<uint64_t>(), &total, 0));
+    if (total != m.nnz)
+        return gs::fail(GS_ERR_INVALID, "COM headers cover %llu positions, nnz is %u",
+                        (unsigned long long)total, m.nnz);
+    GS_TRY(rpos.alloc(((size_t)m.nrows + 1) * 4));
+    k_narrow<<<(m.nrows + 256) / 256, 256>>>(m.nrows + 1, P.as<uint64_t>(), rpos.as<uint32_t>());
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------------ I/O and statistics
+str_matCSR matrixReading(const char *matFileName)
+{
+    str_matCSR m;
+    memset(&m, 0, sizeof(m));
+    if (!matFileName) return m;
+    snprintf(m.name, sizeof(m.name), "%s", matFileName);
+    const char *kind = strstr(matFileName, ".csr") ? "csr" : (strstr(matFileName, ".bin") ? "bin" : nullptr);
+    if (!kind) {
+        printf("\nmatrixReading detected that %s has NOT .csr or .bin extension\n\n", matFileName);
+        gs::fail(GS_ERR_INVALID, "%s has neither a .csr nor a .bin extension", matFileName);
+        return m;
+    }
+    FILE *fh = fopen(matFileName, kind[0] == 'c' ? "r" : "rb");
+    if (!fh) {
+        printf("\nmatrixReading is unable to open .%s file\n\n", kind);
+        gs::fail(GS_ERR_INVALID, "cannot open %s", matFileName);
+        return m;
+    }
+    bool ok = true;
+    UIN n = 0, nnz = 0;
+    if (kind[0] == 'c') {
+        ok = fscanf(fh, "%u %u", &n, &nnz) == 2;
+    } else {
+        ok = fread(&n, sizeof(UIN), 1, fh) == 1 && fread(&nnz, sizeof(UIN), 1, fh) == 1;
+    }
+    if (ok) {
+        m.nrows = n;
+        m.nnz = nnz;
+        m.val = (FPT *)malloc((size_t)(nnz ? nnz : 1) * sizeof(FPT));
+        m.col = (UIN *)malloc((size_t)(nnz ? nnz : 1) * sizeof(UIN));
+        m.row = (UIN *)malloc(((size_t)n + 1) * sizeof(UIN));
+        m.rl = (UIN *)malloc((size_t)(n ? n : 1) * sizeof(UIN));
+        ok = m.val && m.col && m.row && m.rl;
+    }
+    if (ok && kind[0] == 'c') {
+        for (UIN i = 0; ok && i < nnz; i++) ok = fscanf(fh, "%lf %u", &m.val[i], &m.col[i]) == 2;
+        for (UIN i = 0; ok && i <= n; i++) ok = fscanf(fh, "%u", &m.row[i]) == 1;
+    } else if (ok) {
+        ok = fread(m.val, sizeof(FPT), nnz, fh) == nnz && fread(m.col, sizeof(UIN), nnz, fh) == nnz &&
+             fread(m.row, sizeof(UIN), (size_t)n + 1, fh) == (size_t)n + 1;
+    }
+    fclose(fh);
+    if (!ok) {
+        printf("\nmatrixReading failed to parse %s\n\n", matFileName);
+        gs::fail(GS_ERR_INVALID, "malformed matrix file %s", matFileName);
+        free(m.val); free(m.col); free(m.row); free(m.rl);
+        memset(&m, 0, sizeof(m));
+    }
+    return m;
+}
+
+int matrixWritingBin(const char *matFileName, const str_matCSR *m)
+{
+    if (!matFileName || !m) return -1;
+    FILE *fh = fopen(matFileName, "wb");
+    if (!fh) return -1;
+    bool ok = fwrite(&m->nrows, sizeof(UIN), 1, fh) == 1 && fwrite(&m->nnz, sizeof(UIN), 1, fh) == 1 &&
+              fwrite(m->val, sizeof(FPT), m->nnz, fh) == m->nnz &&
+              fwrite(m->col, sizeof(UIN), m->nnz, fh) == m->nnz &&
+              fwrite(m->row, sizeof(UIN), (size_t)m->nrows + 1, fh) == (size_t)m->nrows + 1;
+    return (fclose(fh) == 0 && ok) ? 0 : -1;
+}
+
+void printMatrixStats(const char *matFileName, str_matCSR *m)
+{
+    UIN rmin = 1000000000u, rmax = 0, bw = 0;
+    double s1 = 0.0, s2 = 0.0;
+    for (UIN i = 0; i < m->nrows; i++) {
+        const UIN l = m->row[i + 1] - m->row[i];
+        m->rl[i] = l;
+        s1 += l;
+        s2 += (double)(UIN)(l * l);  // 32-bit square, as cudaSpmv.cu:342
+        rmin = l < rmin ? l : rmin;
+        rmax = l > rmax ? l : rmax;
+        for (UIN j = m->row[i]; j < m->row[i + 1]; j++) {
+            int d = abs((int)i - (int)m->col[j]);
+            if ((UIN)d > bw) bw = (UIN)d;
+        }
+    }
+    s1 /= (double)m->nrows;
+    s2 /= (double)m->nrows;
+    const double sd = sqrt(s2 - s1 * s1);
+    m->rmin = rmin;
+    m->rave = s1;
+    m->rmax = rmax;
+    m->rsd = sd;
+    m->bw = bw;
+    // "<file name up to its first '.'>.sta", next to the matrix file
+    char path[512];
+    snprintf(path, sizeof(path), "%s", matFileName ? matFileName : "matrix");
+    char *slash = strrchr(path, '/');
+    char *dot = strchr(slash ? slash + 1 : path, '.');
+    if (dot) *dot = 0;
+    strncat(path, ".sta", sizeof(path) - strlen(path) - 1);
+    FILE *fh = fopen(path, "w+");
+    if (!fh) return;
+    fprintf(fh, "------------------------------------\n");
+    fprintf(fh, "matrix's statistics\n");
+    fprintf(fh, "------------------------------------\n");
+    fprintf(fh, "name:  %28s\n", matFileName ? matFileName : "");
+    fprintf(fh, "nrows: %28d\n", m->nrows);
+    fprintf(fh, "nnz:   %28d\n", m->nnz);
+    fprintf(fh, "rmin:  %28d\n", m->rmin);
+    fprintf(fh, "rave:  %28.2lf\n", m->rave);
+    fprintf(fh, "rmax:  %28d\n", m->rmax);
+    fprintf(fh, "rsd:   %28.2lf\n", m->rsd);
+    fprintf(fh, "rsdp:  %28.2lf\n", (sd / s1) * 100);
+    fprintf(fh, "bw:    %28d\n", m->bw);
+    fclose(fh);
+}
+
+str_formatData getFormatDataCSR(str_matCSR *m)
+{
+    str_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    m->rowStart = (UIN *)calloc(m->nrows ? m->nrows : 1, sizeof(UIN));
+    m->rowEnd = (UIN *)calloc(m->nrows ? m->nrows : 1, sizeof(UIN));
+    struct timespec t1, t2;
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    for (UIN i = 0; i < m->nrows; i++) {
+        m->rowStart[i] = m->row[i];
+        m->rowEnd[i] = m->row[i + 1];
+    }
+    clock_gettime(CLOCK_MONOTONIC, &t2);
+    strcpy(fd.name, "fcsr");
+    fd.mfp = (double)m->nnz * sizeof(FPT) + (double)m->nnz * sizeof(UIN) +
+             ((double)m->nrows + 1) * sizeof(UIN) + (double)m->nrows * sizeof(FPT);
+    fd.beta = (double)m->nnz / (double)m->nnz;
+    fd.ct = (double)(t2.tv_sec - t1.tv_sec) + (double)(t2.tv_nsec - t1.tv_nsec) * 1e-9;
+    return fd;
+}
+
+void init_vec(const UIN ompNT, const UIN len, FPT *vec)
+{
+    (void)ompNT;
+    for (UIN i = 0; i < len; i++) vec[i] = (FPT)i;
+}
+
+void get_errors(const UIN len, const FPT *ar, const FPT *ac, str_err *e)
+{
+    double md = 0.0, mv = 0.0;
+    UIN pos = 0;
+    for (UIN i = 0; i < len; i++) {
+        const double v = fabs(ar[i]);
+        if (v > mv) mv = v;
+        const double d = fabs(fabs(ac[i]) - v);
+        if (d > md) { md = d; pos = i; }
+    }
+    e->aErr = md;
+    e->rErr = md / mv;
+    e->pos = pos;
+}
+
+void ncsr(const UIN ompNT, const str_matCSR m, const FPT *vec, FPT *res)
+{
+    (void)ompNT;
+    DevBuf row, col, val, x, y;
+    if (h2d(row, m.row, (size_t)m.nrows + 1) || h2d(col, m.col, m.nnz) ||
+        h2d(val, m.val, m.nnz) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8) ||
+        gs_csr_spmv_f64(m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(), val.as<double>(),
+                        x.as<double>(), y.as<double>(), nullptr) ||
+        cudaMemcpy(res, y.p, (size_t)m.nrows * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        fflush(stdout);
+        printf("ncsr: %s\n", gs_last_error());
+        fflush(stdout);
+    }
+}
+
+// ------------------------------------------------------------------ converters
+static gs_status upload_csr(const str_matCSR &m, DevBuf &row, DevBuf &col, DevBuf &val)
+{
+    GS_TRY(h2d(row, m.row, (size_t)m.nrows + 1));
+    GS_TRY(h2d(col, m.col, m.nnz));
+    GS_TRY(h2d(val, m.val, m.nnz));
+    return GS_OK;
+}
+
+str_formatData getFormatDataK1(const UIN blockSize, const str_matCSR m, const FPT *vec,
+                               str_matK1 *k)
+{
+    (void)blockSize;
+    (void)vec;
+    DevBuf row, col, val;
+    gs_matrix A;
+    gs_convert_params p{};
+    p.format = GS_FMT_K1;
+    p.vtype = GS_F64;
+    p.itype = GS_IDX_U32;
+    p.keep_layout = 1;
+    if (upload_csr(m, row, col, val) ||
+        gs::convert(&A, p, m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(), val.p, GS_F64,
+                    nullptr, nullptr, 0))
+        return error_fd("getFormatDataK1");
+    k->nrows = m.nrows;
+    k->nnz = m.nnz;
+    k->chunkNum = A.chunkNum;
+    k->lenVC = A.lenVC;
+    k->permi = d2h_calloc<UIN>(A.permi.p, ((size_t)A.chunkNum + 1) * 32);
+    k->nmc = d2h_calloc<UIN>(A.nmc.p, A.chunkNum);
+    k->chp = d2h_calloc<UIN>(A.chp.p, A.chunkNum);
+    k->val = d2h_calloc<FPT>(A.val.p, A.lenVC);
+    k->col = d2h_calloc<UIN>(A.col.p, A.lenVC);
+    str_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    strcpy(fd.name, "fk1");
+    fd.mfp = A.mfp;
+    fd.beta = A.beta;
+    fd.ct = A.conv_ms * 1e-3;
+    return fd;
+}
+
+str_formatData getFormatDataAXC(const UIN ompNT, const UIN hbs, const str_matCSR m,
+                                const FPT *vec, str_matAXC *a)
+{
+    (void)ompNT;
+    DevBuf row, col, val, x, ax;
+    gs_matrix A;
+    gs_convert_params p{};
+    p.format = GS_FMT_AXC;
+    p.hbs = hbs;
+    p.vtype = GS_F64;
+    p.itype = GS_IDX_U32;
+    p.keep_layout = 1;
+    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) ||
+        gs::convert(&A, p, m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(), val.p, GS_F64,
+                    x.as<double>(), &ax, 0))
+        return error_fd("getFormatDataAXC");
+    a->nrows = m.nrows;
+    a->nnz = m.nnz;
+    a->hbs = hbs;
+    a->lenAX = A.lenAX;
+    a->lenBRP = A.lenBRP;
+    a->lenMAPX = A.lenMAPX;
+    a->ax = d2h_calloc<FPT>(ax.p, A.lenAX);
+    a->brp = d2h_calloc<UIN>(A.brp.p, A.lenBRP);
+    a->mapx = d2h_calloc<UIN>(A.mapx.p, A.lenMAPX);
+    str_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    strcpy(fd.name, "faxc");
+    fd.mfp = A.mfp;
+    fd.beta = A.beta;
+    fd.ct = A.conv_ms * 1e-3;
+    return fd;
+}
+
+str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, const UIN th,
+                                const char *mode, const str_matCSR m, const FPT *vec,
+                                str_matAXT *a)
+{
+    (void)ompNT;
+    const bool unc = mode && (strcmp(mode, "UNC") == 0 || strcmp(mode, "NOC") == 0);
+    const bool com = mode && strcmp(mode, "COM") == 0;
+    if (!unc && !com) {
+        gs::fail(GS_ERR_INVALID, "mode must be \"UNC\" (or \"NOC\") or \"COM\"");
+        return error_fd("getFormatDataAXT");
+    }
+    DevBuf row, col, val, x, ax;
+    gs_matrix A;
+    gs_convert_params p{};
+    p.format = GS_FMT_AXT;
+    p.tileHW = thw;
+    p.tileH = th;
+    p.bs = bs;
+    p.mode = unc ? GS_AXT_UNC : GS_AXT_COM;
+    p.vtype = GS_F64;
+    p.itype = GS_IDX_U32;
+    p.keep_layout = 1;
+    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) ||
+        gs::convert(&A, p, m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(), val.p, GS_F64,
+                    x.as<double>(), &ax, 0))
+        return error_fd("getFormatDataAXT");
+    snprintf(a->name, sizeof(a->name), "%s", m.name);
+    a->nrows = m.nrows;
+    a->nnz = m.nnz;
+    snprintf(a->mode, sizeof(a->mode), "%s", mode);
+    a->tileHW = thw;
+    a->tileH = th;
+    a->logTH = A.logTH;
+    a->tileN = A.tileN;
+    a->lenAX = A.lenAX;
+    a->lenSEC = A.lenSEC;
+    a->lenCON = A.lenCON;
+    a->log = A.log;
+    a->bs = bs;
+    a->ax = d2h_calloc<FPT>(ax.p, A.lenAX);
+    a->sec = d2h_calloc<UIN>(A.sec.p, A.lenSEC);
+    a->con = d2h_calloc<UIN>(A.con.p, (size_t)A.lenCON + 1);
+    str_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    if (unc && th == 1) snprintf(fd.name, sizeof(fd.name), "faxtuh1hw%u", thw);
+    else if (unc) snprintf(fd.name, sizeof(fd.name), "faxtuh%uhw%u", th, thw);
+    else if (th == 1) snprintf(fd.name, sizeof(fd.name), "faxtch1hw%ubs%u", thw, bs);
+    else snprintf(fd.name, sizeof(fd.name), "faxtch%uhw%u", th, thw);
+    fd.mfp = A.mfp;
+    fd.beta = A.beta;
+    fd.ct = A.conv_ms * 1e-3;
+    return fd;
+}
+
+// ------------------------------------------------------------------ entry points
+str_res test_gcsr(const UIN cudaBlockSize, const str_matCSR m, const FPT *vec, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    DevBuf row, col, val, x, y;
+    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8))
+        return error_res("gcsr", gs_last_error());
+    return timed("gcsr", m.nrows, m.nnz, [&]() {
+        return gs_csr_spmv_f64(m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(),
+                               val.as<double>(), x.as<double>(), y.as<double>(), nullptr);
+    }, y, ref);
+}
+
+str_res test_gcucsr(const str_matCSR m, const FPT *vec, const FPT *ref)
+{
+    DevBuf row, col, val, x, y, buf;
+    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8))
+        return error_res("gcucsr", gs_last_error());
+    cusparseHandle_t h = nullptr;
+    cusparseSpMatDescr_t A = nullptr;
+    cusparseDnVecDescr_t vx = nullptr, vy = nullptr;
+    const double one = 1.0, zero = 0.0;
+    size_t bsz = 0;
+    if (cusparseCreate(&h) != CUSPARSE_STATUS_SUCCESS ||
+        cusparseCreateCsr(&A, m.nrows, m.nrows, m.nnz, row.p, col.p, val.p, CUSPARSE_INDEX_32I,
+                          CUSPARSE_INDEX_32I, CUSPARSE_INDEX_BASE_ZERO, CUDA_R_64F) !=
+            CUSPARSE_STATUS_SUCCESS ||
+        cusparseCreateDnVec(&vx, m.nrows, x.p, CUDA_R_64F) != CUSPARSE_STATUS_SUCCESS ||
+        cusparseCreateDnVec(&vy, m.nrows, y.p, CUDA_R_64F) != CUSPARSE_STATUS_SUCCESS ||
+        cusparseSpMV_bufferSize(h, CUSPARSE_OPERATION_NON_TRANSPOSE, &one, A, vx, &zero, vy,
+                                CUDA_R_64F, CUSPARSE_SPMV_ALG_DEFAULT, &bsz) !=
+            CUSPARSE_STATUS_SUCCESS ||
+        buf.alloc(bsz)) {
+        if (vy) cusparseDestroyDnVec(vy);
+        if (vx) cusparseDestroyDnVec(vx);
+        if (A) cusparseDestroySpMat(A);
+        if (h) cusparseDestroy(h);
+        return error_res("gcucsr", "cuSPARSE set-up failed");
+    }
+    str_res r = timed("gcucsr", m.nrows, m.nnz, [&]() -> gs_status {
+        return cusparseSpMV(h, CUSPARSE_OPERATION_NON_TRANSPOSE, &one, A, vx, &zero, vy,
+                            CUDA_R_64F, CUSPARSE_SPMV_ALG_DEFAULT, buf.p) == CUSPARSE_STATUS_SUCCESS
+                   ? GS_OK
+                   : gs::fail(GS_ERR_CUDA, "cusparseSpMV failed");
+    }, y, ref);
+    cusparseDestroyDnVec(vy);
+    cusparseDestroyDnVec(vx);
+    cusparseDestroySpMat(A);
+    cusparseDestroy(h);
+    return r;
+}
+
+str_res test_gk1(const UIN cudaBlockSize, const str_matK1 k, const FPT *vec, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    DevBuf permi, nmc, chp, val, col, x, y, uc, ub, part, cnt;
+    uint32_t units = 0;
+    if (h2d(permi, k.permi, ((size_t)k.chunkNum + 1) * 32) || h2d(nmc, k.nmc, k.chunkNum) ||
+        h2d(chp, k.chp, k.chunkNum) || h2d(val, k.val, k.lenVC) || h2d(col, k.col, k.lenVC) ||
+        h2d(x, vec, k.nrows) || y.alloc((size_t)k.nrows * 8) ||
+        gs::build_k1_plan(nmc.as<UIN>(), k.chunkNum, uc, ub, part, cnt, &units, 0))
+        return error_res("gk1", gs_last_error());
+    gs::K1Args a{};
+    a.nrows = k.nrows;
+    a.chunkNum = k.chunkNum;
+    a.permi = permi.as<UIN>();
+    a.nmc = nmc.as<UIN>();
+    a.chp = chp.as<UIN>();
+    a.klen = nullptr;  // struct carries no row lengths: read each chunk's padded width
+    a.val = val.as<double>();
+    a.col = col.as<UIN>();
+    a.x = x.as<double>();
+    a.y = y.as<double>();
+    a.unit_chunk = uc.as<UIN>();
+    a.unit_base = ub.as<UIN>();
+    a.units = units;
+    a.partial = part.as<double>();
+    a.count = cnt.as<UIN>();
+    return timed("gk1", k.nrows, k.nnz, [&]() { return gs::launch_k1(a, 0); }, y, ref);
+}
+
+static str_res run_baked(const char *name, UIN nrows, UIN nnz, const FPT *hax, UIN lenAX,
+                         DevBuf &rpos, bool tiled, UIN thw, UIN th, UIN axw, const FPT *ref)
+{
+    DevBuf ax, y;
+    if (h2d(ax, hax, lenAX) || y.alloc((size_t)nrows * 8)) return error_res(name, gs_last_error());
+    gs::RowsArgs a{};
+    a.nrows = nrows;
+    a.rpos = rpos.as<UIN>();
+    a.rlen = nullptr;
+    a.val = ax.p;
+    a.col = nullptr;
+    a.x = nullptr;
+    a.y = y.p;
+    a.thw = thw;
+    a.th = th;
+    a.axw = axw;
+    a.nslots = lenAX / 2;
+    const uint32_t lane_pos = tiled ? th : 4;
+    uint64_t positions = 0;
+    UIN last = 0;
+    cudaMemcpy(&last, rpos.as<UIN>() + nrows, 4, cudaMemcpyDeviceToHost);
+    positions = last;
+    const uint32_t rpu = gs::choose_rpu(nrows, positions, lane_pos);
+    return timed(name, nrows, nnz, [&]() {
+        return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, tiled, true, lane_pos, rpu, 0);
+    }, y, ref);
+}
+
+str_res test_gaxc(const UIN cudaBlockSize, const str_matAXC m, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    DevBuf brp, rpos;
+    if (m.hbs == 0) return error_res("gaxc", "hbs is 0");
+    if (h2d(brp, m.brp, m.lenBRP) || rpos.alloc(((size_t)m.nrows + 1) * 4))
+        return error_res("gaxc", gs_last_error());
+    k_div_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows + 1, brp.as<UIN>(), 2, rpos.as<UIN>());
+    return run_baked("gaxc", m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.hbs, 1, m.hbs, ref);
+}
+
+static str_res test_unc1(const char *base, UIN wpw, const str_matAXT m, const FPT *ref)
+{
+    char name[48];
+    snprintf(name, sizeof(name), "%s%u", base, wpw);
+    if (strcmp(m.mode, "UNC") != 0 && strcmp(m.mode, "NOC") != 0)
+        return error_res(name, "matrix is not an UNC AXT layout");
+    if (m.tileH != 1) return error_res(name, "tileH must be 1");
+    DevBuf con, rpos;
+    if (h2d(con, m.con, (size_t)m.lenCON + 1) || rpos.alloc(((size_t)m.nrows + 1) * 4))
+        return error_res(name, gs_last_error());
+    k_div_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows + 1, con.as<UIN>(), 2, rpos.as<UIN>());
+    return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.tileHW, 1, m.tileHW, ref);
+}
+
+str_res test_gaxtuh1hw16w(const UIN wpw, const UIN cbs, const str_matAXT m, const FPT *ref)
+{
+    (void)cbs;
+    return test_unc1("gaxtuh1hw16w", wpw, m, ref);
+}
+str_res test_gaxtuh1hw08w(const UIN wpw, const UIN cbs, const str_matAXT m, const FPT *ref)
+{
+    (void)cbs;
+    return test_unc1("gaxtuh1hw08w", wpw, m, ref);
+}
+str_res test_gaxtuh1hw04w(const UIN wpw, const UIN cbs, const str_matAXT m, const FPT *ref)
+{
+    (void)cbs;
+    return test_unc1("gaxtuh1hw04w", wpw, m, ref);
+}
+
+str_res test_gaxtuh(const UIN tpw, const UIN cbs, const str_matAXT m, const FPT *ref)
+{
+    (void)cbs;
+    char name[48];
+    snprintf(name, sizeof(name), "gaxtuh%utpw%u", m.tileH, tpw);
+    if (strcmp(m.mode, "UNC") != 0 && strcmp(m.mode, "NOC") != 0)
+        return error_res(name, "matrix is not an UNC AXT layout");
+    if (m.tileH < 2) return error_res(name, "tileH must be > 1");
+    DevBuf con, rpos;
+    if (h2d(con, m.con, (size_t)m.lenCON + 1) || rpos.alloc(((size_t)m.nrows + 1) * 4))
+        return error_res(name, gs_last_error());
+    k_unc_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows, con.as<UIN>(), m.tileHW, m.tileH,
+                                                m.tileN, rpos.as<UIN>());
+    return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, true, m.tileHW, m.tileH,
+                     m.tileHW, ref);
+}
+
+static str_res test_com(const char *name, const str_matAXT m, const FPT *ref)
+{
+    if (strcmp(m.mode, "COM") != 0) return error_res(name, "matrix is not a COM AXT layout");
+    DevBuf sec, rpos;
+    if (h2d(sec, m.sec, m.lenSEC) || com_rpos(m, sec, rpos)) return error_res(name, gs_last_error());
+    return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, m.tileH > 1, m.tileHW, m.tileH,
+                     m.tileHW, ref);
+}
+
+str_res test_gaxtch1(const UIN cudaBlockSize, const str_matAXT m, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    char name[48];
+    snprintf(name, sizeof(name), "gaxtch1bs%u", m.bs);
+    if (m.tileH != 1) return error_res(name, "tileH must be 1");
+    return test_com(name, m, ref);
+}
+
+str_res test_gaxtch(const UIN cudaBlockSize, const str_matAXT m, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    char name[48];
+    snprintf(name, sizeof(name), "gaxtch%u", m.tileH);
+    if (m.tileH < 2) return error_res(name, "tileH must be > 1");
+    return test_com(name, m, ref);
+}
+
+}  // extern "C"

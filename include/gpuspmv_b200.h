@@ -1,0 +1,330 @@
+/*
+ * gpuspmv_b200.h -- C ABI of the B200 SpMV engine.
+ *
+ * Two layers, both plain C (no CUDA or torch types in any signature; streams are passed
+ * as an opaque pointer that holds a cudaStream_t):
+ *
+ *  1. Drop-in layer.  The format structs, converters and per-format SpMV entry points of
+ *     the reference program (edoardoCB/gpu_spmv, canonical source cudaSpmv.cu, built with
+ *     FP_TYPE=FP_DOUBLE as its gc.sh does), with the same names, argument meaning and
+ *     struct layouts, so that a driver written against cudaSpmv.cu links against this
+ *     library unchanged.  The converters run on the GPU and return bit-identical host
+ *     arrays; the entry points run sm_100a kernels.  Differences in error behaviour: the
+ *     reference prints and exit()s; this library never exits -- it prints the same kind of
+ *     message, marks the result (name "error", times 0) and records the reason for
+ *     gs_last_error().
+ *
+ *  2. Native layer (gs_*).  Device-resident matrices built on the GPU from a device CSR,
+ *     status-returning, stream-ordered SpMV / SpMM / adjoint calls on device pointers.
+ *
+ * Index type is the reference's UIN (32-bit unsigned) throughout, so every length is
+ * below 2^32.
+ */
+#ifndef GPUSPMV_B200_H
+#define GPUSPMV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================================
+ * 1. Drop-in layer (reference: cudaSpmv.cu)
+ * ==================================================================================== */
+
+typedef unsigned int UIN; /* cudaSpmv.cu:78-80 */
+typedef double FPT;       /* cudaSpmv.cu:64-74 with FP_TYPE == FP_DOUBLE */
+
+/* cudaSpmv.cu:261 */
+typedef struct {
+    char name[48];
+    UIN nrows;
+    UIN nnz;
+    UIN rmin;
+    FPT rave;
+    UIN rmax;
+    FPT rsd;
+    UIN bw;
+    FPT *val;
+    UIN *row;
+    UIN *rowStart;
+    UIN *rowEnd;
+    UIN *col;
+    UIN *rl;
+} str_matCSR;
+
+/* cudaSpmv.cu:385 */
+typedef struct {
+    char name[48];
+    double mfp;
+    double beta;
+    double ct;
+} str_formatData;
+
+/* cudaSpmv.cu:470 */
+typedef struct {
+    double aErr;
+    double rErr;
+    UIN pos;
+} str_err;
+
+/* cudaSpmv.cu:499 */
+typedef struct {
+    char name[48];
+    double et;
+    double ot;
+    double flops;
+    str_err sErr;
+} str_res;
+
+/* cudaSpmv.cu:712 */
+typedef struct {
+    UIN nrows;
+    UIN nnz;
+    UIN chunkNum;
+    UIN lenVC;
+    UIN *permi;
+    UIN *nmc;
+    UIN *chp;
+    FPT *val;
+    UIN *col;
+} str_matK1;
+
+/* cudaSpmv.cu:933 */
+typedef struct {
+    UIN nrows;
+    UIN nnz;
+    UIN hbs;
+    UIN lenAX;
+    UIN lenBRP;
+    UIN lenMAPX;
+    FPT *ax;
+    UIN *brp;
+    UIN *mapx;
+} str_matAXC;
+
+/* cudaSpmv.cu:1154 */
+typedef struct {
+    char name[48];
+    UIN nrows;
+    UIN nnz;
+    char mode[8];
+    UIN tileHW;
+    UIN tileH;
+    UIN logTH;
+    UIN tileN;
+    UIN lenAX;
+    UIN lenSEC;
+    UIN lenCON;
+    UIN log;
+    UIN bs;
+    FPT *ax;
+    UIN *sec;
+    UIN *con;
+} str_matAXT;
+
+/* Matrix I/O and statistics.
+ * matrixReading replaces cudaSpmv.cu:265-328 (.csr text / .bin raw reader).  On failure
+ * the returned struct has nrows = nnz = 0 and NULL arrays (the reference exits).
+ * printMatrixStats replaces cudaSpmv.cu:332-381: fills rl[] and the statistics and writes
+ * "<name up to the first '.'>.sta". */
+str_matCSR matrixReading(const char *matFileName);
+void printMatrixStats(const char *matFileName, str_matCSR *matCSR);
+/* Writes the reference's raw .bin layout (u32 nrows, u32 nnz, FPT val[nnz], u32 col[nnz],
+ * u32 row[nrows+1]); returns 0 on success.  No counterpart in the reference (which only
+ * reads .bin files); provided so generated matrices can be fed to either program. */
+int matrixWritingBin(const char *matFileName, const str_matCSR *matCSR);
+
+/* cudaSpmv.cu:403-436: rowStart/rowEnd copies of row[] (calloc'd), footprint, beta = 1. */
+str_formatData getFormatDataCSR(str_matCSR *matCSR);
+
+/* cudaSpmv.cu:440-447: vec[i] = i. */
+void init_vec(const UIN ompNT, const UIN len, FPT *vec);
+
+/* cudaSpmv.cu:451-466: res = A vec.  Runs on the GPU (sequential per-row order for short
+ * rows, so results match the reference's CPU loop to the last bit for rows that fit one
+ * lane's share; ompNT is accepted and ignored). */
+void ncsr(const UIN ompNT, const str_matCSR matCSR, const FPT *vec, FPT *res);
+
+/* cudaSpmv.cu:474-495. */
+void get_errors(const UIN len, const FPT *ar, const FPT *ac, str_err *sErr);
+
+/* Converters (cudaSpmv.cu:782, 1004, 1391).  They run on the GPU and fill the struct with
+ * calloc'd host arrays that are bit-identical to the reference's CPU converters (x baked
+ * into ax exactly as the reference does).  matCSR.rl must be filled (printMatrixStats).
+ * fd.ct is the device conversion time in seconds.  The caller frees the arrays with
+ * free(), as with the reference. */
+str_formatData getFormatDataK1(const UIN blockSize, const str_matCSR matCSR, const FPT *vec,
+                               str_matK1 *matK1);
+str_formatData getFormatDataAXC(const UIN ompNT, const UIN hbs, const str_matCSR matCSR,
+                                const FPT *vec, str_matAXC *matAXC);
+str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, const UIN th,
+                                const char *mode, const str_matCSR matCSR, const FPT *vec,
+                                str_matAXT *matAXT);
+
+/* Per-format SpMV entry points (cudaSpmv.cu:547, 629, 871, 1100, 1603, 1714, 1854, 1963,
+ * 2101, 2213).  Each copies the host struct to the device, times NUM_ITE launches of the
+ * engine's kernel for that format with CUDA events, copies y back and scores it against
+ * ref with get_errors.  NUM_ITE defaults to 250 (cudaSpmv.cu:96-98) and is set with
+ * gs_set_num_ite().  The launch-shape arguments (cudaBlockSize, wpw, tpw) name the result
+ * as in the reference; the engine picks its own B200 launch shape. */
+str_res test_gcsr(const UIN cudaBlockSize, const str_matCSR matCSR, const FPT *vec,
+                  const FPT *ref);
+str_res test_gcucsr(const str_matCSR matCSR, const FPT *vec, const FPT *ref);
+str_res test_gk1(const UIN cudaBlockSize, const str_matK1 matK1, const FPT *vec,
+                 const FPT *ref);
+str_res test_gaxc(const UIN cudaBlockSize, const str_matAXC matAXC, const FPT *ref);
+str_res test_gaxtuh1hw16w(const UIN wpw, const UIN cbs, const str_matAXT matAXT,
+                          const FPT *ref);
+str_res test_gaxtuh1hw08w(const UIN wpw, const UIN cbs, const str_matAXT matAXT,
+                          const FPT *ref);
+str_res test_gaxtuh1hw04w(const UIN wpw, const UIN cbs, const str_matAXT matAXT,
+                          const FPT *ref);
+str_res test_gaxtuh(const UIN tpw, const UIN cbs, const str_matAXT matAXT, const FPT *ref);
+str_res test_gaxtch1(const UIN cudaBlockSize, const str_matAXT matAXT, const FPT *ref);
+str_res test_gaxtch(const UIN cudaBlockSize, const str_matAXT matAXT, const FPT *ref);
+
+/* ======================================================================================
+ * 2. Native layer
+ * ==================================================================================== */
+
+typedef int gs_status;
+#define GS_OK 0
+#define GS_ERR_INVALID 1     /* bad argument / malformed input */
+#define GS_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define GS_ERR_ALLOC 3       /* device or host allocation failed */
+#define GS_ERR_OVERFLOW 4    /* a 32-bit length or packed header would overflow */
+#define GS_ERR_UNSUPPORTED 5 /* parameter combination not supported */
+#define GS_ERR_DEVICE 6      /* a kernel reported an error through its status word */
+
+typedef enum { GS_F64 = 0, GS_F32 = 1, GS_BF16 = 2 } gs_dtype;
+typedef enum { GS_IDX_U32 = 0, GS_IDX_U16 = 1 } gs_itype;
+typedef enum { GS_FMT_CSR = 0, GS_FMT_K1 = 1, GS_FMT_AXC = 2, GS_FMT_AXT = 3 } gs_format;
+typedef enum { GS_AXT_UNC = 0, GS_AXT_COM = 1 } gs_axt_mode;
+
+/* Opaque handle for a cudaStream_t (NULL = the legacy default stream). */
+typedef void *gs_stream;
+
+const char *gs_status_string(gs_status s);
+/* Text of the most recent error raised on the calling thread ("" if none). */
+const char *gs_last_error(void);
+/* Library version string. */
+const char *gs_version(void);
+/* Number of timed launches used by the drop-in test_* entry points (default 250). */
+void gs_set_num_ite(UIN num_ite);
+UIN gs_get_num_ite(void);
+
+/* Conversion parameters for gs_matrix_create.
+ *  format  : GS_FMT_CSR / K1 / AXC / AXT
+ *  tileHW, tileH, bs, mode : AXT tile half-width, tile height, COM header block size and
+ *            mode -- the arguments of getFormatDataAXT (cudaSpmv.cu:1391)
+ *  hbs     : AXC brick half-size (getFormatDataAXC, cudaSpmv.cu:1004)
+ *  vtype   : stored value type (GS_F64 / GS_F32 / GS_BF16)
+ *  itype   : stored column type (GS_IDX_U32, or GS_IDX_U16 = 16-bit offsets from a 32-bit
+ *            base per 32-row block; conversion fails with GS_ERR_UNSUPPORTED if a block's
+ *            column spread exceeds 65535)
+ *  keep_layout : keep the reference layout's metadata (sec, con, mapx) on the device so
+ *            it can be read back and compared with the reference converters. */
+typedef struct {
+    gs_format format;
+    UIN tileHW;
+    UIN tileH;
+    UIN bs;
+    gs_axt_mode mode;
+    UIN hbs;
+    gs_dtype vtype;
+    gs_itype itype;
+    UIN keep_layout;
+} gs_convert_params;
+
+typedef struct gs_matrix gs_matrix;
+
+/* Build a device-resident matrix from a device CSR (row[nrows+1], col[nnz], val[nnz] of
+ * type val_type).  Runs on `stream`; returns after the conversion has completed. */
+gs_status gs_matrix_create(gs_matrix **out, const gs_convert_params *params, UIN nrows,
+                           UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
+                           const void *d_val, gs_dtype val_type, gs_stream stream);
+gs_status gs_matrix_destroy(gs_matrix *A);
+
+/* Sizes and device arrays of a converted matrix (pointers stay owned by the matrix). */
+typedef struct {
+    gs_format format;
+    UIN nrows, ncols, nnz;
+    /* AXT (str_matAXT fields) */
+    UIN tileHW, tileH, logTH, tileN, lenAX, lenSEC, lenCON, log, bs;
+    gs_axt_mode mode;
+    /* AXC (str_matAXC fields) */
+    UIN hbs, lenBRP, lenMAPX;
+    /* K1 (str_matK1 fields) */
+    UIN chunkNum, lenVC;
+    /* native streams: nslots value/column slots in the format's slot order; slot s of an
+     * AXT/AXC layout is the value half of ax[(s/w)*2w + s%w], w = tileHW or hbs */
+    UIN nslots;
+    gs_dtype vtype;
+    gs_itype itype;
+    const void *d_val;
+    const void *d_col;
+    const UIN *d_colbase; /* per 32-row block column base (GS_IDX_U16 only) */
+    const UIN *d_sec, *d_con, *d_brp, *d_mapx, *d_permi, *d_nmc, *d_chp;
+    /* row table used by the kernels: first position of each row (nrows+1) and real
+     * lengths (NULL when rows are unpadded) */
+    const UIN *d_rpos;
+    const UIN *d_rlen;
+    double conv_ms; /* device time of the conversion */
+    double mfp;     /* memory footprint as the reference counts it (bytes) */
+    double beta;    /* occupancy nnz / stored slots */
+} gs_matrix_info;
+gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *info);
+
+/* Algorithmic (format-independent) bytes of one SpMV with k right-hand sides:
+ * nnz*(s_v+s_i) + 4*(nrows+1) + s_x*ncols*k + s_y*nrows*k. */
+double gs_algorithmic_bytes(UIN nrows, UIN ncols, UIN nnz, UIN k, UIN s_v, UIN s_i, UIN s_x,
+                            UIN s_y);
+
+/* SpMV flags */
+#define GS_FLAG_NONE 0u
+#define GS_FLAG_ACC_F64 1u /* FP32-stored values: FP32 products, FP64 row reduction */
+
+/* y = A x on the device.  x has ncols entries of xtype, y nrows entries of ytype.
+ * F64 matrices take F64 x/y; F32/BF16 matrices take F32 x and F32 or F64 y.
+ * Deterministic: every y entry is written once, with a fixed summation order. */
+gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y,
+                  gs_dtype ytype, UIN flags, gs_stream stream);
+
+/* Same product through host buffers: copies x to the device, runs gs_spmv, copies y
+ * back, all on `stream`, and returns when y is on the host.  d_xbuf/d_ybuf are
+ * caller-provided device staging buffers (ncols / nrows elements). */
+gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dtype xtype,
+                       void *h_y, void *d_ybuf, gs_dtype ytype, UIN flags, gs_stream stream);
+
+/* Synchronous device -> host copy of `bytes` bytes (for bindings that read a matrix's
+ * device arrays back without a CUDA runtime of their own). */
+gs_status gs_copy_to_host(void *h_dst, const void *d_src, size_t bytes);
+
+/* CSR SpMV straight from device CSR arrays (no conversion step): y = A x, FP64. */
+gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
+                          const double *d_val, const double *d_x, double *d_y,
+                          gs_stream stream);
+
+/* Synthetic matrices (host, deterministic for a given seed, any thread count).  Each
+ * returns a CSR in malloc'd host arrays the caller frees with gs_free_host. */
+gs_status gs_gen_laplacian2d(UIN grid, UIN **row, UIN **col, double **val, UIN *nrows,
+                             UIN *nnz);
+gs_status gs_gen_powerlaw(UIN nrows, uint64_t target_nnz, double mu, double sigma,
+                          UIN max_len, uint64_t seed, UIN **row, UIN **col, double **val,
+                          UIN *nnz);
+gs_status gs_gen_stencil27(UIN grid, uint64_t seed, UIN **row, UIN **col, double **val,
+                           UIN *nrows, UIN *nnz);
+gs_status gs_gen_banded(UIN nrows, UIN half_bw, UIN min_len, UIN max_len, uint64_t seed,
+                        UIN **row, UIN **col, double **val, UIN *nnz);
+/* Fill v[0..n) with uniform [lo, hi) (dist 0) or N(0,1) (dist 1). */
+gs_status gs_gen_vector(uint64_t n, int dist, double lo, double hi, uint64_t seed,
+                        double *v);
+void gs_free_host(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUSPMV_B200_H */

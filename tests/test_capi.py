@@ -1,0 +1,93 @@
+"""The C ABI library loads here (no GPU), exports every function include/gpuspmv_b200.h
+declares, and its struct layouts match the header (checked with a host C compiler)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from gpu_spmv_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gpuspmv_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    src = re.sub(r"#[^\n]*", "", src)
+    src = re.sub(r"typedef\s+struct\s*\{.*?\}\s*\w+\s*;", "", src, flags=re.S)
+    src = re.sub(r"typedef[^;]*;", "", src)
+    names = re.findall(r"\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", src)
+    return sorted(set(names))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = L.lib()
+    names = declared_functions()
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(L.SIGNATURES), set(names) - set(L.SIGNATURES)
+
+
+def test_version_and_status_strings():
+    lib = L.lib()
+    assert b"sm_100a" in lib.gs_version()
+    assert lib.gs_status_string(L.GS_ERR_OVERFLOW) == b"GS_ERR_OVERFLOW"
+    lib.gs_set_num_ite(7)
+    assert lib.gs_get_num_ite() == 7
+    lib.gs_set_num_ite(250)
+
+
+def test_argument_errors_need_no_gpu():
+    lib = L.lib()
+    h = C.c_void_p()
+    assert lib.gs_matrix_create(C.byref(h), None, 1, 1, 0, None, None, None, 0, None) == \
+        L.GS_ERR_INVALID
+    assert lib.gs_spmv(None, None, 0, None, 0, 0, None) == L.GS_ERR_INVALID
+    assert lib.gs_matrix_get_info(None, None) == L.GS_ERR_INVALID
+    assert b"NULL" in lib.gs_last_error()
+
+
+@pytest.mark.parametrize("case,expect", [
+    # BASELINE algorithmic bytes: nnz(s_v+s_i) + 4(n+1) + s_x n k + s_y n k
+    ((262144, 262144, 1308672, 1, 8, 4, 8, 8), 20946948),
+    ((4194304, 4194304, 67108864, 1, 8, 4, 8, 8), 889192452),
+    ((4096000, 4096000, 109215352, 1, 8, 4, 8, 8), 1392504228),
+    ((4096000, 4096000, 109215352, 1, 4, 4, 4, 4), 922874820),
+    ((4096000, 4096000, 109215352, 1, 2, 2, 4, 4), 486013412),
+    ((1048576, 1048576, 16777216, 8, 4, 4, 4, 4), 205520900),
+])
+def test_algorithmic_bytes(case, expect):
+    assert L.lib().gs_algorithmic_bytes(*case) == expect
+
+
+def test_struct_layouts_match_header(tmp_path):
+    prog = tmp_path / "sz.c"
+    structs = ["str_matCSR", "str_formatData", "str_err", "str_res", "str_matK1",
+               "str_matAXC", "str_matAXT", "gs_convert_params", "gs_matrix_info"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
+             "int main(void){"]
+    for s in structs:
+        lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
+    lines.append('printf("axt_ax %zu\\n", offsetof(str_matAXT, ax));')
+    lines.append('printf("res_sErr %zu\\n", offsetof(str_res, sErr));')
+    lines.append('printf("info_conv %zu\\n", offsetof(gs_matrix_info, conv_ms));')
+    lines.append("return 0;}")
+    prog.write_text("\n".join(lines))
+    exe = tmp_path / "sz"
+    subprocess.run(["gcc", str(prog), "-o", str(exe)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                  check=True).stdout.splitlines())
+    ct = {"str_matCSR": L.StrMatCSR, "str_formatData": L.StrFormatData, "str_err": L.StrErr,
+          "str_res": L.StrRes, "str_matK1": L.StrMatK1, "str_matAXC": L.StrMatAXC,
+          "str_matAXT": L.StrMatAXT, "gs_convert_params": L.ConvertParams,
+          "gs_matrix_info": L.MatrixInfo}
+    for s, cls in ct.items():
+        assert int(out[s]) == C.sizeof(cls), s
+    assert int(out["axt_ax"]) == L.StrMatAXT.ax.offset
+    assert int(out["res_sErr"]) == L.StrRes.sErr.offset
+    assert int(out["info_conv"]) == L.MatrixInfo.conv_ms.offset

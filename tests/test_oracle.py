@@ -1,0 +1,121 @@
+"""The CPU oracle is pinned before anything is checked against it:
+  * the C restatement (oracle/spmv_oracle.c) reproduces the golden fixtures that the
+    reference's own compiled code produced (tests/golden/*.npz), bit for bit;
+  * where oracle/_ref is built, the restatement equals the live reference on every test
+    matrix and every converter parameter set.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from mats import AXT_PARAMS, CASES, case
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _slots_of(ax_len, w):
+    s = np.arange(ax_len // 2)
+    return (s // w) * 2 * w + s % w
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_port_matches_golden(port, path):
+    g = np.load(path)
+    row, col, val, x = g["row"], g["col"], g["val"], g["x"]
+    n = len(row) - 1
+    xi = np.arange(n, dtype=np.float64)
+    # CPU CSR SpMV: exact (same operation order, no FMA)
+    assert np.array_equal(port.csr_spmv(row, col, val, x), g["y_ncsr"])
+    assert np.array_equal(port.csr_spmv(row, col, val, x), g["y_cpuSpmvCSR"])
+    assert np.array_equal(port.csr_spmv(row, col, val, xi), g["y_ncsr_xi"])
+    rl, st = port.row_stats(row, col)
+    assert np.array_equal(rl, g["rl"])
+    assert np.allclose([st["rmin"], st["rave"], st["rmax"], st["rsd"], st["bw"]], g["stats"],
+                       rtol=0, atol=0)
+    k = port.k1(row, col, val)
+    for f in ("permi", "nmc", "chp", "val", "col"):
+        assert np.array_equal(k[f], g[f"k1_{f}"]), f
+    a = port.axc(row, col, val, x=xi, hbs=32)
+    for f in ("brp", "ax", "mapx"):
+        assert np.array_equal(a[f], g[f"axc_{f}"]), f
+    for (mode, th, thw, bs) in AXT_PARAMS:
+        key = f"axt_{mode}_{th}_{thw}_{bs}"
+        t = port.axt(row, col, val, thw, th, mode, bs=bs, x=xi)
+        d = t["dims"]
+        assert [d.tileN, d.lenAX, d.lenSEC, d.lenCON, d.log, d.logTH] == list(g[key + "_dims"])
+        assert np.array_equal(t["ax"], g[key + "_ax"]), key
+        assert np.array_equal(t["sec"], g[key + "_sec"]), key
+        assert np.array_equal(t["con"], g[key + "_con"]), key
+        # native streams are the two halves of ax (x half == column index when x[i] = i)
+        idx = _slots_of(len(t["ax"]), thw)
+        assert np.array_equal(t["val"], g[key + "_ax"][idx])
+        assert np.array_equal(t["col"].astype(np.float64), g[key + "_ax"][idx + thw])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_port_matches_live_reference(port, ref, name, rng):
+    row, col, val = case(name, np.random.default_rng(sum(map(ord, name))))
+    n = len(row) - 1
+    ncols = max(n, int(col.max()) + 1 if len(col) else n)
+    if ncols != n:
+        pytest.skip("reference converters assume square matrices")
+    xi = ref.init_vec(n)
+    x = rng.uniform(-1, 1, n)
+    assert np.array_equal(port.csr_spmv(row, col, val, x), ref.ncsr(row, col, val, x))
+    k, kr = port.k1(row, col, val), ref.k1(row, col, val, xi)
+    for f in ("permi", "nmc", "chp", "val", "col"):
+        assert np.array_equal(k[f], kr[f]), f
+    a, ar = port.axc(row, col, val, x=xi), ref.axc(row, col, val, xi)
+    for f in ("brp", "ax", "mapx"):
+        assert np.array_equal(a[f], ar[f]), f
+    for (mode, th, thw, bs) in AXT_PARAMS:
+        t = port.axt(row, col, val, thw, th, mode, bs=bs, x=xi)
+        tr = ref.axt(row, col, val, xi, thw, th, mode, bs=bs)
+        for f in ("ax", "sec", "con"):
+            assert np.array_equal(t[f], tr[f]), (mode, th, thw, bs, f)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_port_layout_spmv_consistent(port, name, rng):
+    """Every restated layout computes A x (within FP64 reordering error)."""
+    row, col, val = case(name, np.random.default_rng(1 + sum(map(ord, name))))
+    n = len(row) - 1
+    ncols = max(n, int(col.max()) + 1 if len(col) else n)
+    x = rng.uniform(-1, 1, ncols)
+    y_true, mag = port.csr_truth(row, col, val, x)
+    k = port.k1(row, col, val)
+    assert np.all(np.abs(port.k1_spmv(k, x) - y_true) <= 1e-13 * mag + 0.0)
+    for (mode, th, thw, bs) in AXT_PARAMS:
+        if mode == "COM" and (th & (th - 1)):
+            continue
+        t = port.axt(row, col, val, thw, th, mode, bs=bs, x=x)
+        assert np.all(np.abs(port.axt_spmv(t, x) - y_true) <= 1e-13 * mag), (mode, th, thw)
+        assert np.all(np.abs(port.axt_spmv_baked(t) - y_true) <= 1e-13 * mag), (mode, th, thw)
+
+
+def test_k1_permutation_is_stable_descending(port, rng):
+    lens = rng.integers(0, 6, 4000)  # many ties
+    from mats import csr_from_lengths
+
+    row, col, val = csr_from_lengths(lens, 4000, rng)
+    k = port.k1(row, col, val)
+    p = k["permi"][:4000]
+    rl = np.diff(row)[p]
+    assert np.all(rl[:-1] >= rl[1:])
+    ties = rl[:-1] == rl[1:]
+    assert np.all(p[:-1][ties] < p[1:][ties])
+
+
+def test_com_row0_header_is_zero(port):
+    """The layout fact behind the reference defect in gaxtch1 (cudaSpmv.cu:2089): when row
+    0 has one element, its COM header word is 0 and indistinguishable from 'no header'
+    unless the decoder knows every segment block starts with a header."""
+    row = np.array([0, 1, 3, 6], np.uint32)
+    col = np.array([0, 0, 2, 0, 1, 2], np.uint32)
+    val = np.arange(1, 7, dtype=np.float64)
+    t = port.axt(row, col, val, 32, 1, "COM", bs=4)
+    assert t["sec"][0] == 0
+    x = np.array([1.0, 2.0, 3.0])
+    assert np.array_equal(port.axt_spmv(t, x), port.csr_spmv(row, col, val, x))
