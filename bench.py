@@ -59,9 +59,15 @@ VARIANTS = {
     "axt-unc-th1-hw4": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
     "axt-unc-th1-hw8": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=8),
     "axt-unc-th1-hw16": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=16),
+    "axt-com-th16": dict(fmt="AXT", mode="COM", tileH=16, tileHW=32, bs=256),
     "axt-unc-th2": dict(fmt="AXT", mode="UNC", tileH=2, tileHW=32),
     "axt-unc-th4": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
     "axt-unc-th8": dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
+    # kernel variants of the same layouts (comparison / tuning)
+    "axt-com-th8-tma": dict(fmt="AXT", mode="COM", tileH=8, tileHW=32, bs=256, tma=True),
+    "axt-unc-th4-tma": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32, tma=True),
+    "axt-com-th1-striped": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256,
+                                striped=True),
 }
 DEFAULT_VARIANT = "axt-com-th1"
 
@@ -265,17 +271,20 @@ def run_ours(args):
     variants = list(VARIANTS) if args.sweep else [args.variant]
     results = {}
     for vname in variants:
-        A = E.Matrix(row, col, val, ncols=n, **VARIANTS[vname])
+        kw = dict(VARIANTS[vname])
+        tma = kw.pop("tma", False)
+        striped = kw.pop("striped", False)
+        A = E.Matrix(row, col, val, ncols=n, **kw)
         dx = torch.from_numpy(x).cuda()
         dy = torch.empty(n, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream()
         for _ in range(args.warmup):
-            A.spmv(dx, dy)
+            A.spmv(dx, dy, tma=tma, striped=striped)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         K = args.steps
-        sampler = ClockSampler(local) if (rank == 0 and not args.sweep) else None
+        sampler = ClockSampler(local) if (rank == 0 and not args.sweep and not args.no_clocks) else None
         if sampler:
             sampler.start()
             time.sleep(0.3)
@@ -286,19 +295,21 @@ def run_ours(args):
         ev0.record(stream)
         for k in range(K):
             eb[k].record(stream)
-            A.spmv(dx, dy)
+            A.spmv(dx, dy, tma=tma, striped=striped)
             ea[k].record(stream)
         ev1.record(stream)
         torch.cuda.synchronize()
         if sampler:
             sampler.stop()
+        if A.device_status():
+            raise RuntimeError(f"{vname}: a kernel reported a timed-out wait")
         elapsed = ev0.elapsed_time(ev1)  # ms
         kern = sum(b.elapsed_time(a) for b, a in zip(eb, ea)) / K
         if dist:
             t = torch.tensor([elapsed, kern], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             elapsed, kern = float(t[0]), float(t[1])
-        results[vname] = (A, elapsed, kern, sampler, dx, dy)
+        results[vname] = (A, elapsed, kern, sampler, dx, dy, tma, striped)
         if args.sweep and rank == 0:
             gf = 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
             B = E.algorithmic_bytes(n, n, nnz)
@@ -309,7 +320,8 @@ def run_ours(args):
             A.close()
     if args.sweep:
         return 0
-    A, elapsed, kern, sampler, dx, dy = results[args.variant]
+    A, elapsed, kern, sampler, dx, dy, tma, striped = results[args.variant]
+    spmv_flags = (L.GS_FLAG_TMA if tma else 0) | (L.GS_FLAG_STRIPED if striped else 0)
     K = args.steps
     value = world * 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
     B = E.algorithmic_bytes(n, n, nnz)
@@ -328,14 +340,14 @@ def run_ours(args):
         sh = E.stream_handle()
         for _ in range(3):
             L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
-                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, 0, sh), "e2e")
+                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, spmv_flags, sh), "e2e")
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(Ke):
             L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
-                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, 0, sh), "e2e")
+                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, spmv_flags, sh), "e2e")
         te = time.perf_counter() - t0
         if dist:
             t = torch.tensor([te], dtype=torch.float64, device="cuda")
@@ -395,6 +407,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -25,7 +25,7 @@ GS_F64, GS_F32, GS_BF16 = 0, 1, 2
 GS_IDX_U32, GS_IDX_U16 = 0, 1
 GS_FMT_CSR, GS_FMT_K1, GS_FMT_AXC, GS_FMT_AXT = 0, 1, 2, 3
 GS_AXT_UNC, GS_AXT_COM = 0, 1
-GS_FLAG_NONE, GS_FLAG_ACC_F64 = 0, 1
+GS_FLAG_NONE, GS_FLAG_ACC_F64, GS_FLAG_TMA, GS_FLAG_STRIPED = 0, 1, 2, 4
 
 
 # ------------------------------------------------------------------ drop-in structs
@@ -128,6 +128,7 @@ SIGNATURES = {
     "gs_spmv_host": (_st, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_int, UIN, _vp]),
     "gs_csr_spmv_f64": (_st, [UIN, UIN, UIN, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gs_copy_to_host": (_st, [_vp, _vp, C.c_size_t]),
+    "gs_matrix_device_status": (_st, [_vp, C.POINTER(UIN), C.c_int]),
     "gs_gen_laplacian2d": (_st, [UIN, C.POINTER(UINp), C.POINTER(UINp), C.POINTER(FPTp),
                                  C.POINTER(UIN), C.POINTER(UIN)]),
     "gs_gen_powerlaw": (_st, [UIN, C.c_uint64, C.c_double, C.c_double, UIN, C.c_uint64,

@@ -146,20 +146,18 @@ gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y
     if (f64 && xtype != GS_F64) return gs::fail(GS_ERR_UNSUPPORTED, "FP64 matrices take FP64 x");
     if (!f64 && xtype != GS_F32)
         return gs::fail(GS_ERR_UNSUPPORTED, "FP32/BF16 matrices take FP32 x");
-    gs::RowsArgs a{};
-    a.nrows = A->nrows;
-    a.rpos = A->rpos.as<uint32_t>();
-    a.rlen = A->rlen.as<uint32_t>();
+    gs::RowsArgs a = gs::rows_args(A->plan);
     a.val = A->val.p;
     a.col = A->col.p;
-    a.colbase = A->colbase.as<uint32_t>();
     a.x = d_x;
     a.y = d_y;
-    a.thw = A->tileHW ? A->tileHW : 1;
-    a.th = A->tileH ? A->tileH : 1;
+    if (A->tiled) {
+        a.thw = A->tileHW;
+        a.th = A->tileH;
+    }
     a.nslots = A->nslots;
     return gs::launch_rows(a, A->p.vtype, A->p.itype, ytype, flags, A->tiled != 0, false,
-                           A->lane_pos, A->rpu, s);
+                           A->plan.padded, s);
 }
 
 gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dtype xtype,
@@ -174,6 +172,17 @@ gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dty
     GS_CUDA(cudaMemcpyAsync(h_y, d_ybuf, (size_t)A->nrows * gs::dtype_size(ytype),
                             cudaMemcpyDeviceToHost, s));
     GS_CUDA(cudaStreamSynchronize(s));
+    return GS_OK;
+}
+
+gs_status gs_matrix_device_status(const gs_matrix *A, UIN *word, int reset)
+{
+    if (!A || !word) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    *word = 0;
+    if (!A->plan.status.p) return GS_OK;
+    GS_CUDA(cudaDeviceSynchronize());
+    GS_CUDA(cudaMemcpy(word, A->plan.status.p, 4, cudaMemcpyDeviceToHost));
+    if (reset) GS_CUDA(cudaMemset(A->plan.status.p, 0, 4));
     return GS_OK;
 }
 
@@ -195,19 +204,18 @@ gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const
         return gs::fail(GS_ERR_INVALID, "NULL argument");
     if ((reinterpret_cast<uintptr_t>(d_val) & 15u) || (reinterpret_cast<uintptr_t>(d_col) & 15u))
         return gs::fail(GS_ERR_INVALID, "val and col must be 16-byte aligned");
-    gs::RowsArgs a{};
-    a.nrows = nrows;
-    a.rpos = d_row;
-    a.rlen = nullptr;
+    cudaStream_t s = gs::cs(stream);
+    gs::RowsPlan P;
+    GS_TRY(gs::build_rows_plan(d_row, nullptr, nrows, gs::kDirectV, P, s));
+    gs::RowsArgs a = gs::rows_args(P);
     a.val = d_val;
     a.col = d_col;
     a.x = d_x;
     a.y = d_y;
-    a.thw = 1;
-    a.th = 1;
     a.nslots = nnz;
-    return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, false, false, 4,
-                           gs::choose_rpu(nrows, nnz, 4), gs::cs(stream));
+    GS_TRY(gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, false, false, false, s));
+    GS_CUDA(cudaStreamSynchronize(s));  // the plan's buffers are released on return
+    return GS_OK;
 }
 
 }  // extern "C"

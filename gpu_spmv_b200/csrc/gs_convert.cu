@@ -39,9 +39,8 @@ struct FillArgs {
     int layout, sec_mode;
     uint32_t thw, th, bs, log;
     uint32_t *sec;
-    void *oval, *ocol;
-    const uint32_t *colbase;
-    uint32_t rpu;
+    void *oval;
+    uint32_t *ocol;
     uint32_t *mapx;
     const double *xbake;
     double *ax;
@@ -56,7 +55,7 @@ template <> __device__ __forceinline__ double cvt<float, double>(float v) { retu
 template <> __device__ __forceinline__ float cvt<float, float>(float v) { return v; }
 template <> __device__ __forceinline__ __nv_bfloat16 cvt<float, __nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
-template <class VIN, class VOUT, class IOUT>
+template <class VIN, class VOUT>
 __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
 {
     const int lane = threadIdx.x & 31;
@@ -64,10 +63,9 @@ __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const VIN *val = static_cast<const VIN *>(f.val);
     VOUT *oval = static_cast<VOUT *>(f.oval);
-    IOUT *ocol = static_cast<IOUT *>(f.ocol);
+    uint32_t *ocol = f.ocol;
     for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < f.n; r += warps) {
         const uint32_t b = f.row[r], len = f.row[r + 1] - b;
-        const uint32_t base = (sizeof(IOUT) == 2) ? f.colbase[r / f.rpu] : 0u;
         for (uint32_t e = lane; e < len; e += 32) {
             const uint32_t p = b + e;
             const VIN v = val[p];
@@ -89,7 +87,7 @@ __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
                 }
             }
             if (oval) oval[slot] = cvt<VIN, VOUT>(v);
-            if (ocol) ocol[slot] = (IOUT)(c - base);
+            if (ocol) ocol[slot] = c;
             if (f.sec_mode == kSecTile) {
                 if (e % f.thw == 0) f.sec[slot / f.thw] = r;
             } else if (f.sec_mode == kSecColumn) {
@@ -184,31 +182,6 @@ __global__ void k_validate(uint32_t n, uint32_t ncols, uint32_t nnz, const uint3
     if (bad) atomicOr(flag, bad);
 }
 
-// per unit of rpu rows: minimum column (base of the 16-bit offsets); flag if spread > 65535
-__global__ void k_colbase(uint32_t n, uint32_t rpu, const uint32_t *row, const uint32_t *col,
-                          uint32_t *colbase, uint32_t *flag)
-{
-    const int lane = threadIdx.x & 31;
-    const uint32_t units = (n + rpu - 1) / rpu;
-    for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < units;
-         u += gridDim.x * (blockDim.x >> 5)) {
-        const uint32_t r0 = u * rpu, r1 = min(n, r0 + rpu);
-        uint32_t mn = 0xffffffffu, mx = 0;
-        for (uint32_t p = row[r0] + lane; p < row[r1]; p += 32) {
-            mn = min(mn, col[p]);
-            mx = max(mx, col[p]);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        }
-        if (lane == 0) {
-            colbase[u] = (mn == 0xffffffffu) ? 0u : mn;
-            if (mn != 0xffffffffu && mx - mn > 65535u) atomicOr(flag, 4u);
-        }
-    }
-}
-
 inline unsigned blocks_for(uint64_t n, unsigned t = 256) { return (unsigned)((n + t - 1) / t); }
 
 uint32_t ref_log_loop(uint32_t v, uint32_t from, uint32_t to_excl)
@@ -219,20 +192,14 @@ uint32_t ref_log_loop(uint32_t v, uint32_t from, uint32_t to_excl)
 }
 
 template <class VIN>
-gs_status launch_fill(const FillArgs &f, gs_dtype vout, gs_itype iout, cudaStream_t s)
+gs_status launch_fill(const FillArgs &f, gs_dtype vout, cudaStream_t s)
 {
     const uint64_t want = ((uint64_t)f.n + 7) / 8;
     unsigned blocks = (unsigned)(want < 148u * 64u ? want : 148u * 64u);
     if (blocks == 0) return GS_OK;
-    if (iout == GS_IDX_U16) {
-        if (vout == GS_F32) k_fill<VIN, float, uint16_t><<<blocks, 256, 0, s>>>(f);
-        else if (vout == GS_BF16) k_fill<VIN, __nv_bfloat16, uint16_t><<<blocks, 256, 0, s>>>(f);
-        else return fail(GS_ERR_UNSUPPORTED, "16-bit columns need FP32 or BF16 values");
-    } else {
-        if (vout == GS_F64) k_fill<VIN, double, uint32_t><<<blocks, 256, 0, s>>>(f);
-        else if (vout == GS_F32) k_fill<VIN, float, uint32_t><<<blocks, 256, 0, s>>>(f);
-        else k_fill<VIN, __nv_bfloat16, uint32_t><<<blocks, 256, 0, s>>>(f);
-    }
+    if (vout == GS_F64) k_fill<VIN, double><<<blocks, 256, 0, s>>>(f);
+    else if (vout == GS_F32) k_fill<VIN, float><<<blocks, 256, 0, s>>>(f);
+    else k_fill<VIN, __nv_bfloat16><<<blocks, 256, 0, s>>>(f);
     GS_CHECK_LAUNCH();
     return GS_OK;
 }
@@ -289,7 +256,6 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
     f.col = d_col;
     f.val = d_val;
     f.xbake = d_xbake;
-    f.rpu = 32;
     DevBuf P;  // 64-bit offsets
     const gs_format fmt = p.format;
 
@@ -478,45 +444,48 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
             k_rowlen<<<blocks_for(n), 256, 0, s>>>(n, d_row, A->rlen.as<uint32_t>());
             GS_CHECK_LAUNCH();
         }
-        A->lane_pos = reduced ? 8 : 4;
-        // positions per row drive the rows-per-unit choice; the tiled layouts walk th per lane
-        const uint64_t positions = A->tiled ? (uint64_t)A->nslots : (uint64_t)A->nslots;
-        A->rpu = choose_rpu(n, positions, A->tiled ? th : A->lane_pos);
-        // ---- value / column streams
-        const size_t vsz = dtype_size(p.vtype), isz = p.itype == GS_IDX_U16 ? 2 : 4;
-        GS_TRY(A->val.alloc_zero((size_t)A->nslots * vsz, s));
-        GS_TRY(A->col.alloc_zero((size_t)A->nslots * isz, s));
-        if (p.itype == GS_IDX_U16) {
-            if (A->tiled) return fail(GS_ERR_UNSUPPORTED, "16-bit columns need tileH=1");
-            const uint32_t units = (n + A->rpu - 1) / A->rpu;
-            GS_TRY(A->colbase.alloc((size_t)units * 4));
-            DevBuf flag;
-            GS_TRY(flag.alloc_zero(4, s));
-            k_colbase<<<(units + 7) / 8, 256, 0, s>>>(n, A->rpu, d_row, d_col,
-                                                      A->colbase.as<uint32_t>(),
-                                                      flag.as<uint32_t>());
-            GS_CHECK_LAUNCH();
-            uint32_t hf = 0;
-            GS_CUDA(cudaMemcpyAsync(&hf, flag.p, 4, cudaMemcpyDeviceToHost, s));
-            GS_CUDA(cudaStreamSynchronize(s));
-            if (hf & 4u)
-                return fail(GS_ERR_UNSUPPORTED,
-                            "a %u-row block spans more than 65536 columns: 16-bit column "
-                            "offsets do not fit this matrix",
-                            A->rpu);
-            f.colbase = A->colbase.as<uint32_t>();
-            f.rpu = A->rpu;
-        }
+        // ---- value / column streams (32-bit columns first; narrowed below for U16)
+        if (p.itype == GS_IDX_U16 && A->tiled)
+            return fail(GS_ERR_UNSUPPORTED, "16-bit columns need tileH=1");
+        GS_TRY(A->val.alloc_zero((size_t)A->nslots * dtype_size(p.vtype), s));
+        DevBuf col32;
+        DevBuf &c32 = (p.itype == GS_IDX_U16) ? col32 : A->col;
+        GS_TRY(c32.alloc_zero((size_t)A->nslots * 4, s));
         f.rpos = (f.layout == kCom) ? d_row : A->rpos.as<uint32_t>();
         f.oval = A->val.p;
-        f.ocol = A->col.p;
+        f.ocol = c32.as<uint32_t>();
         if (ax_out) {
-            const uint32_t lenax = fmt == GS_FMT_AXC ? A->lenAX : A->lenAX;
-            GS_TRY(ax_out->alloc_zero((size_t)lenax * 8, s));
+            GS_TRY(ax_out->alloc_zero((size_t)A->lenAX * 8, s));
             f.ax = ax_out->as<double>();
         }
-        if (val_type == GS_F64) GS_TRY(launch_fill<double>(f, p.vtype, p.itype, s));
-        else GS_TRY(launch_fill<float>(f, p.vtype, p.itype, s));
+        if (val_type == GS_F64) GS_TRY(launch_fill<double>(f, p.vtype, s));
+        else GS_TRY(launch_fill<float>(f, p.vtype, s));
+        // ---- execution plan of the row-stream kernel.  Rows of the UNC layouts start on a
+        // tile column (tileH > 1) or a tile (tileH = 1), and AXC rows on a brick: the lane
+        // width V is chosen to divide that alignment so the aligned kernel applies.
+        uint32_t V = kDirectV;
+        bool aligned = false;
+        if (A->tiled) {
+            V = th;
+            aligned = fmt == GS_FMT_AXT && p.mode == GS_AXT_UNC &&
+                      (th == 2 || th == 4 || th == 8 || th == 16);
+        } else if ((fmt == GS_FMT_AXT && p.mode == GS_AXT_UNC) || fmt == GS_FMT_AXC) {
+            const uint32_t align = fmt == GS_FMT_AXC ? p.hbs : thw;
+            if (reduced) {  // reduced-precision kernels use 8 positions per lane
+                aligned = align % 8 == 0;
+            } else {
+                V = aligned_lane_positions(align, &aligned);
+            }
+        }
+        GS_TRY(build_rows_plan(A->rpos.as<uint32_t>(), need_rlen ? A->rlen.as<uint32_t>() : nullptr,
+                               n, V, A->plan, s));
+        A->plan.aligned = aligned;
+        if (p.itype == GS_IDX_U16) {
+            GS_TRY(A->col.alloc_zero((size_t)A->nslots * 2, s));
+            GS_TRY(build_u16_columns(col32.as<uint32_t>(), A->nslots, A->plan,
+                                     A->col.as<uint16_t>(), s));
+            A->colbase.reset();
+        }
     }
 
     GS_CUDA(cudaEventRecord(e1, s));

@@ -68,6 +68,8 @@ enum class CountKind {
     ArrayTimes,     // arr[i] * a
     BitZero,        // (arr[i] >> a) & 1 == 0   (radix sort pass)
     PiecesMin1,     // max(1, ceil(arr[i] / a))
+    WindowPopc,     // popcount of the a words arr[i*a .. i*a+a)
+    NonEmpty,       // row[i+1] > row[i]
 };
 struct CountSpec {
     CountKind kind;
@@ -108,6 +110,23 @@ template <> struct ValTraits<__nv_bfloat16> {
 
 }  // namespace gs
 
+namespace gs {
+// Execution plan of the row-stream kernel (gs_spmv_rows.cu), built once per matrix:
+//  sbits  : bit p set <=> position p is the first position of a non-empty row
+//  rbits  : bit p set <=> position p holds a real element (padded layouts only)
+//  wcount : number of set start bits before each window of 32*V positions
+//  ne     : rank -> row index of the non-empty rows (only when some rows are empty)
+//  empty  : the empty rows (their y entries are written 0)
+//  colbase: per-window base of the 16-bit column offsets (GS_IDX_U16 only)
+//  status : device status word (bit 0: a bounded wait in a kernel timed out)
+//  aligned: every row starts on a multiple of V positions (UNC / AXC layouts)
+struct RowsPlan {
+    uint32_t npos = 0, nwin = 0, V = 8, wpw = 4, n_empty = 0;
+    bool padded = false, aligned = false;
+    DevBuf sbits, rbits, wcount, ne, empty, colbase, status;
+};
+}  // namespace gs
+
 // ------------------------------------------------------------------ the matrix handle
 struct gs_matrix {
     gs_convert_params p{};
@@ -127,32 +146,43 @@ struct gs_matrix {
     gs::DevBuf k1len, k1unit_chunk, k1unit_base, k1partial, k1count;
     uint32_t k1units = 0;
     // row-stream kernel configuration
-    uint32_t tiled = 0;    // 1: positions map to tile slots (tileH > 1 layouts)
-    uint32_t lane_pos = 4; // positions per lane per window
-    uint32_t rpu = 32;     // rows per warp unit
+    uint32_t tiled = 0;  // 1: positions map to tile slots (tileH > 1 layouts)
+    gs::RowsPlan plan;
     double conv_ms = 0, mfp = 0, beta = 0;
 };
 
 namespace gs {
 
-// Row-stream SpMV over a position table (see gs_spmv_rows.cu).
+// Row-stream SpMV (see gs_spmv_rows.cu).
 struct RowsArgs {
-    uint32_t nrows;
-    const uint32_t *rpos;   // nrows+1 first positions
-    const uint32_t *rlen;   // real lengths or nullptr (rows unpadded)
-    const void *val;        // value stream (or baked ax)
-    const void *col;        // column stream (u32 or u16 offsets)
-    const uint32_t *colbase;// per-unit base for u16 offsets
+    uint32_t npos, nwin, wpw, V;   // positions, windows of 32*V positions, windows per warp
+    uint32_t thw, th;              // tile shape of tiled (tileH > 1) layouts
+    uint32_t axw;                  // baked layouts: ax half width (tileHW or hbs)
+    uint32_t nslots;               // length of the value/column streams
+    uint32_t n_empty;
+    uint32_t aligned;              // rows start on multiples of V (aligned kernel applies)
+    const uint32_t *sbits, *rbits, *wcount, *ne, *empty, *colbase;
+    uint32_t *status;  // device status word (bounded-wait timeouts)
+    const void *val;   // value stream (or the baked ax)
+    const void *col;  // column stream (u32, or u16 offsets from colbase)
     const void *x;
     void *y;
-    uint32_t thw, th;       // tile shape for tiled position->slot mapping
-    uint32_t axw;           // baked: ax half width (tileHW or hbs)
-    uint32_t nslots;        // length of the value/column streams (vector loads stop short)
 };
+// Positions per lane of the direct (tileH = 1) layouts.
+constexpr uint32_t kDirectV = 8;
+// Positions per lane for a layout whose rows start on multiples of `align` positions
+// (0: no alignment): returns the V that makes the aligned kernel apply, or kDirectV.
+uint32_t aligned_lane_positions(uint32_t align, bool *aligned);
+// Build the plan from a row table: rpos[0..n] first position of each row (rpos[n] = total
+// positions), rlen[r] real length (nullptr when rows carry no padding).
+gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
+                          uint32_t V, RowsPlan &P, cudaStream_t s);
+// 16-bit column offsets: per-window base over real positions, col16 = col32 - base.
+gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &P,
+                            uint16_t *d_col16, cudaStream_t s);
+RowsArgs rows_args(const RowsPlan &P);
 gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
-                      uint32_t flags, bool tiled, bool baked, uint32_t lane_pos, uint32_t rpu,
-                      cudaStream_t s);
-uint32_t choose_rpu(uint32_t nrows, uint64_t positions, uint32_t lane_pos);
+                      uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s);
 
 // K1 SpMV (see gs_spmv_k1.cu).
 struct K1Args {

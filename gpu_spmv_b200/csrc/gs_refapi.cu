@@ -490,11 +490,18 @@ str_res test_gcsr(const UIN cudaBlockSize, const str_matCSR m, const FPT *vec, c
 {
     (void)cudaBlockSize;
     DevBuf row, col, val, x, y;
-    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8))
+    gs::RowsPlan P;
+    if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8) ||
+        gs::build_rows_plan(row.as<UIN>(), nullptr, m.nrows, gs::kDirectV, P, 0))
         return error_res("gcsr", gs_last_error());
+    gs::RowsArgs a = gs::rows_args(P);
+    a.val = val.p;
+    a.col = col.p;
+    a.x = x.p;
+    a.y = y.p;
+    a.nslots = m.nnz;
     return timed("gcsr", m.nrows, m.nnz, [&]() {
-        return gs_csr_spmv_f64(m.nrows, m.nrows, m.nnz, row.as<UIN>(), col.as<UIN>(),
-                               val.as<double>(), x.as<double>(), y.as<double>(), nullptr);
+        return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, false, false, false, 0);
     }, y, ref);
 }
 
@@ -566,31 +573,35 @@ str_res test_gk1(const UIN cudaBlockSize, const str_matK1 k, const FPT *vec, con
     return timed("gk1", k.nrows, k.nnz, [&]() { return gs::launch_k1(a, 0); }, y, ref);
 }
 
+// align: rows start on multiples of `align` positions (UNC tiles / columns, AXC bricks),
+// 0 for the compact COM layouts.
 static str_res run_baked(const char *name, UIN nrows, UIN nnz, const FPT *hax, UIN lenAX,
-                         DevBuf &rpos, bool tiled, UIN thw, UIN th, UIN axw, const FPT *ref)
+                         DevBuf &rpos, bool tiled, UIN thw, UIN th, UIN axw, UIN align,
+                         const FPT *ref)
 {
     DevBuf ax, y;
-    if (h2d(ax, hax, lenAX) || y.alloc((size_t)nrows * 8)) return error_res(name, gs_last_error());
-    gs::RowsArgs a{};
-    a.nrows = nrows;
-    a.rpos = rpos.as<UIN>();
-    a.rlen = nullptr;
+    gs::RowsPlan P;
+    uint32_t V = tiled ? th : gs::kDirectV;
+    bool aligned = false;
+    if (tiled) aligned = align != 0 && (th == 2 || th == 4 || th == 8 || th == 16);
+    else if (align) V = gs::aligned_lane_positions(align, &aligned);
+    if (h2d(ax, hax, lenAX) || y.alloc((size_t)nrows * 8) ||
+        gs::build_rows_plan(rpos.as<UIN>(), nullptr, nrows, V, P, 0))
+        return error_res(name, gs_last_error());
+    P.aligned = aligned;
+    gs::RowsArgs a = gs::rows_args(P);
     a.val = ax.p;
     a.col = nullptr;
     a.x = nullptr;
     a.y = y.p;
-    a.thw = thw;
-    a.th = th;
+    if (tiled) {
+        a.thw = thw;
+        a.th = th;
+    }
     a.axw = axw;
     a.nslots = lenAX / 2;
-    const uint32_t lane_pos = tiled ? th : 4;
-    uint64_t positions = 0;
-    UIN last = 0;
-    cudaMemcpy(&last, rpos.as<UIN>() + nrows, 4, cudaMemcpyDeviceToHost);
-    positions = last;
-    const uint32_t rpu = gs::choose_rpu(nrows, positions, lane_pos);
     return timed(name, nrows, nnz, [&]() {
-        return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, tiled, true, lane_pos, rpu, 0);
+        return gs::launch_rows(a, GS_F64, GS_IDX_U32, GS_F64, 0, tiled, true, false, 0);
     }, y, ref);
 }
 
@@ -602,7 +613,8 @@ str_res test_gaxc(const UIN cudaBlockSize, const str_matAXC m, const FPT *ref)
     if (h2d(brp, m.brp, m.lenBRP) || rpos.alloc(((size_t)m.nrows + 1) * 4))
         return error_res("gaxc", gs_last_error());
     k_div_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows + 1, brp.as<UIN>(), 2, rpos.as<UIN>());
-    return run_baked("gaxc", m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.hbs, 1, m.hbs, ref);
+    return run_baked("gaxc", m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.hbs, 1, m.hbs, m.hbs,
+                     ref);
 }
 
 static str_res test_unc1(const char *base, UIN wpw, const str_matAXT m, const FPT *ref)
@@ -616,7 +628,8 @@ static str_res test_unc1(const char *base, UIN wpw, const str_matAXT m, const FP
     if (h2d(con, m.con, (size_t)m.lenCON + 1) || rpos.alloc(((size_t)m.nrows + 1) * 4))
         return error_res(name, gs_last_error());
     k_div_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows + 1, con.as<UIN>(), 2, rpos.as<UIN>());
-    return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.tileHW, 1, m.tileHW, ref);
+    return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, false, m.tileHW, 1, m.tileHW,
+                     m.tileHW, ref);
 }
 
 str_res test_gaxtuh1hw16w(const UIN wpw, const UIN cbs, const str_matAXT m, const FPT *ref)
@@ -649,7 +662,7 @@ str_res test_gaxtuh(const UIN tpw, const UIN cbs, const str_matAXT m, const FPT 
     k_unc_table<<<(m.nrows + 256) / 256, 256>>>(m.nrows, con.as<UIN>(), m.tileHW, m.tileH,
                                                 m.tileN, rpos.as<UIN>());
     return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, true, m.tileHW, m.tileH,
-                     m.tileHW, ref);
+                     m.tileHW, m.tileH, ref);
 }
 
 static str_res test_com(const char *name, const str_matAXT m, const FPT *ref)
@@ -658,7 +671,7 @@ static str_res test_com(const char *name, const str_matAXT m, const FPT *ref)
     DevBuf sec, rpos;
     if (h2d(sec, m.sec, m.lenSEC) || com_rpos(m, sec, rpos)) return error_res(name, gs_last_error());
     return run_baked(name, m.nrows, m.nnz, m.ax, m.lenAX, rpos, m.tileH > 1, m.tileHW, m.tileH,
-                     m.tileHW, ref);
+                     m.tileHW, 0, ref);
 }
 
 str_res test_gaxtch1(const UIN cudaBlockSize, const str_matAXT m, const FPT *ref)

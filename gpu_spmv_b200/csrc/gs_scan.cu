@@ -69,10 +69,16 @@ struct CountDev {
         case 2: return (uint64_t)arr[i];
         case 3: return (uint64_t)arr[i] * (uint64_t)a;
         case 4: return (uint64_t)(((arr[i] >> a) & 1u) == 0u);
-        default: {
+        case 5: {
             uint32_t t = (arr[i] + a - 1) / a;
             return (uint64_t)(t ? t : 1u);
         }
+        case 6: {
+            uint64_t c = 0;
+            for (uint32_t j = 0; j < a; j++) c += __popc(arr[i * a + j]);
+            return c;
+        }
+        default: return (uint64_t)(row[i + 1] > row[i]);
         }
     }
 };

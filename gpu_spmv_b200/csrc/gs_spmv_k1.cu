@@ -39,8 +39,23 @@ __global__ void __launch_bounds__(256) k_k1(const K1Args a)
         const uint32_t j1 = min(len, j0 + kK1Split);
         const uint32_t base = __ldg(a.chp + c) + (uint32_t)lane;
         double acc = 0.0;
-#pragma unroll 4
-        for (uint32_t j = j0; j < j1; j++) {
+        uint32_t j = j0;
+        // 8 slots in flight per lane: loads first, then gathers, then the ordered sum
+        for (; j + 8 <= j1; j += 8) {
+            double v[8], xv[8];
+            uint32_t c[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const uint32_t pos = base + 32u * (j + u);
+                v[u] = __ldcs(a.val + pos);
+                c[u] = __ldcs(a.col + pos);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) xv[u] = __ldg(a.x + c[u]);
+#pragma unroll
+            for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, __dmul_rn(v[u], xv[u]));
+        }
+        for (; j < j1; j++) {
             const uint32_t pos = base + 32u * j;
             const double v = __ldcs(a.val + pos);
             const double xv = __ldg(a.x + __ldcs(a.col + pos));

@@ -1,29 +1,40 @@
-// gs_spmv_rows.cu -- the row-stream SpMV kernel shared by CSR, AXC and every AXT layout.
+// gs_spmv_rows.cu -- the row-stream SpMV kernels shared by CSR, AXC and every AXT layout.
 //
-// What it computes is the reference's SpMV for each of those formats:
+// What they compute is the reference's SpMV for each of those formats:
 //   gcsr          cudaSpmv.cu:531-543   (CSR, one thread per row)
 //   gaxc          cudaSpmv.cu:1072-1096 (AXC bricks, one warp per row)
 //   gaxtuh1hw16w/08w/04w cudaSpmv.cu:1570-1850 (AXT UNC tileH=1, tiles summed, atomics)
 //   gaxtuh        cudaSpmv.cu:1939-1959 (AXT UNC tileH>1, column sums, atomics)
 //   gaxtch1       cudaSpmv.cu:2041-2097 (AXT COM tileH=1, block scan over headers)
 //   gaxtch        cudaSpmv.cu:2174-2209 (AXT COM tileH>1, per-column segment walk)
-// but the decomposition is different and the same for all of them:
+// with one decomposition for all of them:
 //
-// * Every layout is described by a row table: rpos[r] = first position of row r in the
-//   layout's position space, rlen[r] = number of real (non-padding) positions (or NULL
-//   when rows are unpadded).  A position maps to a storage slot either directly (CSR,
-//   AXC, tileH=1 AXT: the layout stores each row's elements contiguously) or through the
-//   tile transpose of the tileH>1 layouts (position P -> tile P/(th*thw), tile row P%th,
-//   tile column (P%(th*thw))/th), which is what makes lane-contiguous positions land in
-//   warp-coalesced slots.
-// * One warp owns RPU consecutive rows.  It walks their positions in windows of
-//   32 lanes x V positions; each lane takes V consecutive positions (merge-path style):
-//   vector loads of the value/column streams, independent x gathers (read-only path,
-//   through L2), a sequential per-lane sum with row breaks, then one segmented warp scan
-//   (5 shuffles) joins rows that cross lanes, and a carry joins rows that cross windows.
-// * Padding positions are never multiplied and never loaded when a lane's whole share is
-//   padding.  Every y entry is written exactly once (no atomics, no y pre-zeroing), so the
-//   result is deterministic and one launch is the whole SpMV.
+// * Position space.  Every layout is a sequence of positions in which each row occupies a
+//   contiguous span (CSR and COM: the CSR element order; UNC and AXC: the padded rows).  A
+//   position maps to a storage slot directly (tileH = 1 layouts) or through the tile
+//   transpose of the tileH > 1 layouts (position P -> tile P/(th*thw), tile row P%th, tile
+//   column (P%(th*thw))/th): the lane that owns th consecutive positions then reads one
+//   slot of each tile row, and a warp's 32 lanes read 32 consecutive slots.
+// * Plan (built once at conversion): a bitmap of row starts (1 bit per position), a
+//   bitmap of real positions for padded layouts, and the running count of row starts per
+//   window.  They replace the per-row pointers: a window's row structure is one popcount
+//   scan across the warp.
+// * Work: a warp owns a range of windows of 32 lanes x V positions; a lane takes V
+//   consecutive positions: V independent x gathers through L2 (read-only path), a
+//   sequential per-lane sum with row breaks, one segmented warp scan (5 shuffles) to join
+//   rows that cross lanes, a carry for rows that cross windows.  A row belongs to the warp
+//   in whose range it starts: the warp skips the leading continuation of the previous
+//   warp's row and finishes its own last row past the end of its range.  Every y entry is
+//   written once with a fixed summation order: no atomics, no y zero-fill, deterministic,
+//   one launch per SpMV.
+// * Staging.  k_rows loads the value/column streams with vectorised streaming loads
+//   (direct layouts) or coalesced per-tile-row loads (tiled layouts).  k_rows_tma, for the
+//   tiled layouts with 32-wide tiles, streams whole tiles into a per-warp ring of shared
+//   memory stages with 1-D TMA bulk copies (cp.async.bulk, no multicast) completing on
+//   mbarriers, several tiles ahead of the warp; the L1 then serves only the x gathers,
+//   and lane c reads its tile column at a 32-slot stride (no bank conflicts).  Waits on
+//   the mbarriers are bounded: on timeout the kernel records an error in the status word
+//   and leaves.
 //
 // Baked mode reads the reference layouts with x baked into ax (value half at
 // ax[(s/w)*2w + s%w], x half w further), which is what the drop-in entry points receive.
@@ -38,45 +49,31 @@ namespace gs {
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
+constexpr int kTmaWarps = 4;   // warps per block of the TMA kernel
+constexpr int kTmaStages = 4;  // tiles in flight per warp
 constexpr unsigned kFull = 0xffffffffu;
 
-template <class T> __device__ __forceinline__ T shfl_up(T v, int d) {
-    return __shfl_up_sync(kFull, v, d);
-}
-template <class T> __device__ __forceinline__ T shfl_idx(T v, int l) {
-    return __shfl_sync(kFull, v, l);
-}
-
-// exact product / sum without contraction into FMA (the reference's CPU loop multiplies
-// and adds separately)
+// exact product / sum, never contracted into FMA (the reference's CPU loop multiplies and
+// adds separately)
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
-// ---- streaming loads of V consecutive elements starting at an aligned index
-template <class T, int V> struct VecLoad;
-template <> struct VecLoad<double, 4> {
-    __device__ __forceinline__ static void run(const double *p, double (&o)[4]) {
-        double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
-        double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
-        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-    }
-};
-template <> struct VecLoad<double, 8> {
+// ---- streaming loads of 8 consecutive elements from an 8-element-aligned index
+template <class T> struct Load8;
+template <> struct Load8<double> {
     __device__ __forceinline__ static void run(const double *p, double (&o)[8]) {
         const double2 *q = reinterpret_cast<const double2 *>(p);
 #pragma unroll
-        for (int i = 0; i < 4; i++) { double2 a = __ldcs(q + i); o[2 * i] = a.x; o[2 * i + 1] = a.y; }
+        for (int i = 0; i < 4; i++) {
+            double2 a = __ldcs(q + i);
+            o[2 * i] = a.x;
+            o[2 * i + 1] = a.y;
+        }
     }
 };
-template <> struct VecLoad<float, 4> {
-    __device__ __forceinline__ static void run(const float *p, float (&o)[4]) {
-        float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
-        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-    }
-};
-template <> struct VecLoad<float, 8> {
+template <> struct Load8<float> {
     __device__ __forceinline__ static void run(const float *p, float (&o)[8]) {
         const float4 *q = reinterpret_cast<const float4 *>(p);
         float4 a = __ldcs(q), b = __ldcs(q + 1);
@@ -84,13 +81,7 @@ template <> struct VecLoad<float, 8> {
         o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
     }
 };
-template <> struct VecLoad<uint32_t, 4> {
-    __device__ __forceinline__ static void run(const uint32_t *p, uint32_t (&o)[4]) {
-        uint4 a = __ldcs(reinterpret_cast<const uint4 *>(p));
-        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-    }
-};
-template <> struct VecLoad<uint32_t, 8> {
+template <> struct Load8<uint32_t> {
     __device__ __forceinline__ static void run(const uint32_t *p, uint32_t (&o)[8]) {
         const uint4 *q = reinterpret_cast<const uint4 *>(p);
         uint4 a = __ldcs(q), b = __ldcs(q + 1);
@@ -98,13 +89,7 @@ template <> struct VecLoad<uint32_t, 8> {
         o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
     }
 };
-template <> struct VecLoad<uint16_t, 4> {
-    __device__ __forceinline__ static void run(const uint16_t *p, uint16_t (&o)[4]) {
-        uint2 a = __ldcs(reinterpret_cast<const uint2 *>(p));
-        o[0] = a.x & 0xffff; o[1] = a.x >> 16; o[2] = a.y & 0xffff; o[3] = a.y >> 16;
-    }
-};
-template <> struct VecLoad<uint16_t, 8> {
+template <> struct Load8<uint16_t> {
     __device__ __forceinline__ static void run(const uint16_t *p, uint16_t (&o)[8]) {
         uint4 a = __ldcs(reinterpret_cast<const uint4 *>(p));
         uint32_t w[4] = {a.x, a.y, a.z, a.w};
@@ -112,18 +97,7 @@ template <> struct VecLoad<uint16_t, 8> {
         for (int i = 0; i < 4; i++) { o[2 * i] = w[i] & 0xffff; o[2 * i + 1] = w[i] >> 16; }
     }
 };
-template <> struct VecLoad<__nv_bfloat16, 4> {
-    __device__ __forceinline__ static void run(const __nv_bfloat16 *p, __nv_bfloat16 (&o)[4]) {
-        uint2 a = __ldcs(reinterpret_cast<const uint2 *>(p));
-        uint32_t w[2] = {a.x, a.y};
-#pragma unroll
-        for (int i = 0; i < 2; i++) {
-            o[2 * i] = __ushort_as_bfloat16((unsigned short)(w[i] & 0xffff));
-            o[2 * i + 1] = __ushort_as_bfloat16((unsigned short)(w[i] >> 16));
-        }
-    }
-};
-template <> struct VecLoad<__nv_bfloat16, 8> {
+template <> struct Load8<__nv_bfloat16> {
     __device__ __forceinline__ static void run(const __nv_bfloat16 *p, __nv_bfloat16 (&o)[8]) {
         uint4 a = __ldcs(reinterpret_cast<const uint4 *>(p));
         uint32_t w[4] = {a.x, a.y, a.z, a.w};
@@ -140,290 +114,1228 @@ template <> __device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat
     return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short *>(p)));
 }
 
-template <class T> __device__ __forceinline__ T to_acc(double v);
-template <> __device__ __forceinline__ double to_acc<double>(double v) { return v; }
-template <> __device__ __forceinline__ float to_acc<float>(double v) { return (float)v; }
+template <class YT, class AT> __device__ __forceinline__ void store_y(YT *y, AT v) { *y = (YT)v; }
 
-template <class YT, class AT> __device__ __forceinline__ void store_y(YT *y, AT v) {
-    *y = (YT)v;
+// V bits of a position bitmap starting at position p (V <= 32; the bitmap has two words
+// of zero slack past its last window)
+__device__ __forceinline__ uint32_t get_bits(const uint32_t *bm, uint32_t p, uint32_t V)
+{
+    const uint32_t w = p >> 5, sh = p & 31;
+    const uint64_t two = (uint64_t)__ldg(bm + w) | ((uint64_t)__ldg(bm + w + 1) << 32);
+    return (uint32_t)(two >> sh) & (V >= 32 ? 0xffffffffu : ((1u << V) - 1u));
+}
+
+// ---- TMA bulk copy / mbarrier primitives (1-D bulk copies, no multicast)
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for an mbarrier phase: gives up after ~2 s of wall time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > 2000000000ull) return false;
+    return true;
 }
 
 // ---------------------------------------------------------------------------------------
-// VT value storage, IT column storage (u32 or u16 offsets), XT x type, PT product type,
-// AT accumulation type, YT output type.  VMAX positions per lane (compile time); the
-// runtime lane share is VMAX for direct layouts and th (<= VMAX) for tiled ones.
-template <class VT, class IT, class XT, class PT, class AT, class YT, int VMAX, bool TILED,
-          bool BAKED, int RPU>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-k_rows(const RowsArgs a, const uint32_t nunits)
+// Window control: which of the lane's V positions belong to this warp.  Before the first
+// row start of the warp's range, positions continue an earlier warp's row (skipped); past
+// the range ("over"), only the remainder of the warp's last row counts.
+struct WinCtl {
+    uint32_t vmask;
+    unsigned slanes;  // lanes with a row start among their in-bounds positions
+    bool skip;        // nothing of this window is ours
+};
+
+__device__ __forceinline__ WinCtl window_ctl(int lane, uint32_t W, uint32_t V, uint32_t FULLV,
+                                             uint32_t npos, uint32_t sraw, bool seen, bool over)
 {
-    __shared__ uint32_t s_rps[kWarpsPerBlock][RPU + 1];
-    __shared__ uint32_t s_rre[kWarpsPerBlock][RPU];
+    const uint32_t qb = W + (uint32_t)lane * V;
+    WinCtl c;
+    const uint32_t inb = (qb >= npos) ? 0u
+                         : (qb + V <= npos ? FULLV : ((1u << (npos - qb)) - 1u));
+    c.slanes = __ballot_sync(kFull, (sraw & inb) != 0u);
+    c.vmask = inb;
+    c.skip = false;
+    if (!seen || over) {
+        if (c.slanes == 0u) {
+            if (!seen) c.skip = true;
+        } else {
+            const int fl = __ffs(c.slanes) - 1;
+            const uint32_t fb = __shfl_sync(kFull, sraw & inb, fl);
+            const uint32_t fpos = W + (uint32_t)fl * V + (uint32_t)(__ffs(fb) - 1);
+            const uint32_t ge = (qb >= fpos) ? FULLV
+                                : (qb + V <= fpos ? 0u : ((FULLV << (fpos - qb)) & FULLV));
+            c.vmask = seen ? (c.vmask & ~ge) : (c.vmask & ge);
+        }
+    }
+    return c;
+}
+
+// Row ranks, sequential lane sums, segmented warp scan, y writes and the window carry.
+template <class AT, class YT, int VM, bool EMPTY, class PT>
+__device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane, uint32_t W,
+                                              uint32_t V, uint32_t sraw, uint32_t vmask,
+                                              uint32_t rb, const PT (&prod)[VM], uint32_t &cnt,
+                                              AT &carry)
+{
+    const uint32_t qb = W + (uint32_t)lane * V;
+    const uint32_t sb = sraw & vmask;
+    const int c0 = __popc(sb);
+    int inc = c0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int t = __shfl_up_sync(kFull, inc, d);
+        if (lane >= d) inc += t;
+    }
+    const uint32_t total = (uint32_t)__shfl_sync(kFull, inc, 31);
+    // whether the row in progress at the lane's last position ends there
+    const uint32_t nxt_lane = __shfl_down_sync(kFull, sraw, 1);
+    const uint32_t nxt_win = (lane == 31) ? get_bits(a.sbits, W + 32u * V, 1) : 0u;
+
+    const bool has = vmask != 0u;
+    const int kfirst = has ? __ffs(vmask) - 1 : 0;
+    const int klast = has ? 31 - __clz(vmask) : 0;
+    const bool starts = has && ((sb >> kfirst) & 1u);
+    uint32_t rank = cnt + (uint32_t)(inc - c0) - 1u;  // row in progress before the lane
+    const uint32_t first_rank = rank + (starts ? 1u : 0u);
+    int nb = 0;
+    AT head = (AT)0, acc = (AT)0;
+    // prod[] is +0 outside the real positions of vmask, and a sum that starts at +0 never
+    // changes by adding +0: every position is added without a test
+#pragma unroll
+    for (int k = 0; k < VM; k++) {
+        if (k < (int)V) {
+            if ((sb >> k) & 1u) {
+                if (k != kfirst) {
+                    if (nb == 0) head = acc;
+                    else store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + rank) : rank), acc);
+                    nb++;
+                }
+                rank++;
+                acc = (AT)0;
+            }
+            acc = add_rn(acc, (AT)prod[k]);
+        }
+    }
+    (void)rb;
+    const uint32_t last_rank = rank;
+    bool next_start;
+    if (klast + 1 < (int)V) next_start = (sraw >> (klast + 1)) & 1u;
+    else next_start = (lane < 31) ? (nxt_lane & 1u) : (nxt_win & 1u);
+    if (qb + (uint32_t)klast + 1 >= a.npos) next_start = true;
+    const bool ends = has && next_start;
+
+    const bool rf = has && (nb > 0 || starts);
+    const unsigned rmask = __ballot_sync(kFull, rf);
+    const unsigned le = rmask & (kFull >> (31 - lane));
+    const int sstart = le ? 31 - __clz(le) : -1;
+    AT S = acc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        AT t = __shfl_up_sync(kFull, S, d);
+        if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
+    }
+    if (sstart < 0) S = add_rn(S, carry);
+    AT E = __shfl_up_sync(kFull, S, 1);
+    if (lane == 0) E = carry;
+    if (has) {
+        if (nb > 0)
+            store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + first_rank) : first_rank),
+                            starts ? head : add_rn(head, E));
+        if (ends) store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + last_rank) : last_rank), S);
+    }
+    carry = __shfl_sync(kFull, S, 31);
+    cnt += total;
+}
+
+// Products of the lane's real positions, loaded from global memory (vectorised streaming
+// loads for direct layouts, one coalesced load per tile row for tiled layouts).
+template <class VT, class IT, class XT, class PT, int VM, bool TILED, bool BAKED>
+__device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint32_t qb,
+                                             uint32_t V, uint32_t rb, PT (&prod)[VM])
+{
+    const VT *val = static_cast<const VT *>(a.val);
+    const IT *col = static_cast<const IT *>(a.col);
+    const XT *x = static_cast<const XT *>(a.x);
+    const double *ax = static_cast<const double *>(a.val);
+    const uint32_t ths = a.th * a.thw;
+#pragma unroll
+    for (int k = 0; k < VM; k++) prod[k] = (PT)0;
+    if (!rb) return;
+    if constexpr (BAKED) {
+#pragma unroll
+        for (int k = 0; k < VM; k++) {
+            if (k < (int)V && ((rb >> k) & 1u)) {
+                uint32_t s = qb + k;
+                if constexpr (TILED) {
+                    const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
+                    s = t * ths + (uint32_t)k * a.thw + c;
+                }
+                const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                prod[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
+            }
+        }
+    } else if constexpr (!TILED) {
+        VT v[VM];
+        IT c[VM];
+        if (qb + VM <= a.nslots) {
+            Load8<VT>::run(val + qb, v);
+            Load8<IT>::run(col + qb, c);
+        } else {  // stream tail: element loads, never past the last slot
+#pragma unroll
+            for (int k = 0; k < VM; k++) {
+                v[k] = (VT)0;
+                c[k] = 0;
+                if ((rb >> k) & 1u) {
+                    v[k] = ld_stream(val + qb + k);
+                    c[k] = ld_stream(col + qb + k);
+                }
+            }
+        }
+        const uint32_t cbase = (sizeof(IT) == 2) ? __ldg(a.colbase + w) : 0u;
+        XT xv[VM];
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            xv[k] = ((rb >> k) & 1u) ? __ldg(x + (cbase + (uint32_t)c[k])) : (XT)0;
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            if ((rb >> k) & 1u) prod[k] = mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k]);
+    } else {
+        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
+        const uint32_t s0 = t * ths + cc;
+        VT v[VM];
+        IT c[VM];
+#pragma unroll
+        for (int k = 0; k < VM; k++) {
+            v[k] = (VT)0;
+            c[k] = 0;
+            if (k < (int)V && ((rb >> k) & 1u)) {
+                v[k] = ld_stream(val + s0 + (uint32_t)k * a.thw);
+                c[k] = ld_stream(col + s0 + (uint32_t)k * a.thw);
+            }
+        }
+        XT xv[VM];
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            xv[k] = (k < (int)V && ((rb >> k) & 1u)) ? __ldg(x + (uint32_t)c[k]) : (XT)0;
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            if (k < (int)V && ((rb >> k) & 1u))
+                prod[k] = mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k]);
+    }
+}
+
+// One window's streams as loaded for a lane: start / real bits and the V value / column
+// pairs (baked layouts: value and x halves).  Loaded a window ahead of their use so that
+// the stream latency overlaps the previous window's x gathers.
+template <class VT, class IT, int VM, bool BAKED>
+struct WinData {
+    uint32_t sraw, rraw;
+    VT v[VM];
+    IT c[VM];
+    double xb[BAKED ? VM : 1];
+};
+
+template <class VT, class IT, int VM, bool TILED, bool BAKED, bool PADDED>
+__device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane, uint32_t V,
+                                         WinData<VT, IT, VM, BAKED> &d)
+{
+    const uint32_t qb = w * 32u * V + (uint32_t)lane * V;
+    d.sraw = get_bits(a.sbits, qb, V);
+    d.rraw = PADDED ? get_bits(a.rbits, qb, V) : 0xffffffffu;
+    const VT *val = static_cast<const VT *>(a.val);
+    const IT *col = static_cast<const IT *>(a.col);
+    const uint32_t ths = a.th * a.thw;
+    if constexpr (BAKED) {
+        const double *ax = static_cast<const double *>(a.val);
+#pragma unroll
+        for (int k = 0; k < VM; k++) {
+            d.v[k] = 0.0;
+            d.xb[k] = 0.0;
+            if (k < (int)V && qb + k < a.npos) {
+                uint32_t s = qb + k;
+                if constexpr (TILED) {
+                    const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
+                    s = t * ths + (uint32_t)k * a.thw + cc;
+                }
+                const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                d.v[k] = __ldcs(ax + ai);
+                d.xb[k] = __ldcs(ax + ai + a.axw);
+            }
+        }
+    } else if constexpr (!TILED) {
+        if (qb + VM <= a.nslots) {
+            Load8<VT>::run(val + qb, d.v);
+            Load8<IT>::run(col + qb, d.c);
+        } else {  // stream tail: element loads, never past the last slot
+#pragma unroll
+            for (int k = 0; k < VM; k++) {
+                d.v[k] = (VT)0;
+                d.c[k] = 0;
+                if (qb + k < a.npos) {
+                    d.v[k] = ld_stream(val + qb + k);
+                    d.c[k] = ld_stream(col + qb + k);
+                }
+            }
+        }
+    } else {
+        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
+        const uint32_t s0 = t * ths + cc;
+#pragma unroll
+        for (int k = 0; k < VM; k++) {
+            d.v[k] = (VT)0;
+            d.c[k] = 0;
+            if (k < (int)V && qb + k < a.npos) {
+                d.v[k] = ld_stream(val + s0 + (uint32_t)k * a.thw);
+                d.c[k] = ld_stream(col + s0 + (uint32_t)k * a.thw);
+            }
+        }
+    }
+}
+
+// x gathers and products of the real positions rb of a loaded window (0 elsewhere).
+template <class VT, class IT, class XT, class PT, int VM, bool BAKED>
+__device__ __forceinline__ void win_products(const RowsArgs &a, uint32_t w, uint32_t V,
+                                             const WinData<VT, IT, VM, BAKED> &d, uint32_t rb,
+                                             PT (&prod)[VM])
+{
+    if constexpr (BAKED) {
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            prod[k] = (k < (int)V && ((rb >> k) & 1u)) ? (PT)mul_rn(d.v[k], d.xb[k]) : (PT)0;
+    } else {
+        const XT *x = static_cast<const XT *>(a.x);
+        const uint32_t cbase = (sizeof(IT) == 2) ? __ldg(a.colbase + w) : 0u;
+        XT xv[VM];
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            xv[k] = (k < (int)V && ((rb >> k) & 1u)) ? __ldg(x + (cbase + (uint32_t)d.c[k]))
+                                                      : (XT)0;
+#pragma unroll
+        for (int k = 0; k < VM; k++)
+            prod[k] = (k < (int)V && ((rb >> k) & 1u))
+                          ? mul_rn((PT)ValTraits<VT>::to_f64(d.v[k]), (PT)xv[k])
+                          : (PT)0;
+    }
+}
+
+// Windows from `w` on, past the warp's range end w1, until its last row ends.
+template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY>
+__device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int lane, uint32_t w,
+                                                uint32_t V, uint32_t FULLV, uint32_t cnt,
+                                                AT carry)
+{
+    for (; w < a.nwin; w++) {
+        const uint32_t W = w * 32u * V;
+        const uint32_t qb = W + (uint32_t)lane * V;
+        const uint32_t sraw = get_bits(a.sbits, qb, V);
+        const WinCtl ctl = window_ctl(lane, W, V, FULLV, a.npos, sraw, true, true);
+        const uint32_t rb = PADDED ? (get_bits(a.rbits, qb, V) & ctl.vmask) : ctl.vmask;
+        PT prod[VM];
+        products_ldg<VT, IT, XT, PT, VM, TILED, BAKED>(a, w, qb, V, rb, prod);
+        window_reduce<AT, YT, VM, EMPTY, PT>(a, y, lane, W, V, sraw, ctl.vmask, rb, prod, cnt,
+                                             carry);
+        if (ctl.slanes != 0u) break;  // the last row ended in this window
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// LDG-staged kernel (every layout).  VT value storage, IT column storage (u32 or u16
+// offsets), XT x type, PT product type, AT accumulation type, YT output type.  VM =
+// positions per lane for direct layouts and the upper bound of th for tiled ones.  PADDED:
+// the layout has padding positions (real-bit map).  EMPTY: some rows are empty.
+template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
+{
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    uint32_t *rps = s_rps[wib];
-    uint32_t *rre = s_rre[wib];
+    YT *y = static_cast<YT *>(a.y);
+    const uint32_t V = TILED ? a.th : (uint32_t)VM;
+    const uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
+    const uint32_t WS = 32u * V;
+    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
+    const uint32_t gw = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+
+    if constexpr (EMPTY) {
+        for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
+            store_y<YT, AT>(y + __ldg(a.empty + i), (AT)0);
+    }
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    for (uint32_t rg = gw; rg < nranges; rg += nwarps) {
+        const uint32_t w0 = rg * a.wpw;
+        const uint32_t w1 = min(w0 + a.wpw, a.nwin);
+        uint32_t cnt = __ldg(a.wcount + w0);  // row starts before this range
+        bool seen = (w0 == 0);                // a row start has been met in the range
+        AT carry = (AT)0;
+        for (uint32_t w = w0; w < w1; w++) {
+            // bits and streams are requested together (the streams do not wait for the
+            // bits), then the x gathers
+            WinData<VT, IT, VM, BAKED> cur;
+            load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w, lane, V, cur);
+            const uint32_t W = w * WS;
+            const WinCtl ctl = window_ctl(lane, W, V, FULLV, a.npos, cur.sraw, seen, false);
+            if (ctl.skip) continue;  // all of it continues an earlier warp's row
+            const uint32_t rb = cur.rraw & ctl.vmask;
+            PT prod[VM];
+            win_products<VT, IT, XT, PT, VM, BAKED>(a, w, V, cur, rb, prod);
+            window_reduce<AT, YT, VM, EMPTY, PT>(a, y, lane, W, V, cur.sraw, ctl.vmask, rb,
+                                                 prod, cnt, carry);
+            seen = true;
+        }
+        if (seen)
+            finish_overhang<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, PADDED, EMPTY>(
+                a, y, lane, w1, V, FULLV, cnt, carry);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Aligned kernel.  In the UNC layouts every row starts on a tile column (tileH > 1: a
+// multiple of th positions) or a tile (tileH = 1: a multiple of tileHW), and in AXC on a
+// brick: with V positions per lane and V dividing that alignment, a lane never holds two
+// rows.  Its V products are one partial sum, the window's row starts are one ballot of the
+// lanes' first bits, and a row's lanes are joined by one segmented scan -- close to the
+// instruction count of a row-per-lane kernel while keeping the AXT tile layout's
+// coalesced loads.
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY>
+__global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
+{
+    const int lane = threadIdx.x & 31;
     YT *y = static_cast<YT *>(a.y);
     const VT *val = static_cast<const VT *>(a.val);
     const IT *col = static_cast<const IT *>(a.col);
     const XT *x = static_cast<const XT *>(a.x);
     const double *ax = static_cast<const double *>(a.val);
-    const uint32_t V = TILED ? a.th : (uint32_t)VMAX;
-    const uint32_t WS = 32u * V;
+    constexpr uint32_t WS = 32u * V;
+    constexpr uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
     const uint32_t ths = a.th * a.thw;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const unsigned mine = 0xffffffffu >> (31 - lane);  // lanes 0..lane
 
-    for (uint32_t u = blockIdx.x * kWarpsPerBlock + wib; u < nunits;
-         u += gridDim.x * kWarpsPerBlock) {
-        const uint32_t R0 = u * RPU;
-        const int nr = (int)min((uint32_t)RPU, a.nrows - R0);
-        // ---- row table of the unit
-        for (int i = lane; i <= nr; i += 32) rps[i] = __ldg(a.rpos + R0 + i);
-        __syncwarp();
-        for (int i = lane; i < nr; i += 32) {
-            uint32_t s0 = rps[i], s1 = rps[i + 1];
-            rre[i] = a.rlen ? s0 + __ldg(a.rlen + R0 + i) : s1;
-            if (s0 == s1) store_y<YT, AT>(y + R0 + i, (AT)0);  // empty row
-        }
-        __syncwarp();
-        const uint32_t P0 = rps[0], P1 = rps[nr];
-        const uint32_t cbase = (sizeof(IT) == 2) ? __ldg(a.colbase + u) : 0u;
+    if constexpr (EMPTY) {
+        for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
+            store_y<YT, AT>(y + __ldg(a.empty + i), (AT)0);
+    }
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    for (uint32_t rg = gw; rg < nranges; rg += nwarps) {
+        const uint32_t w0 = rg * a.wpw;
+        const uint32_t w1 = min(w0 + a.wpw, a.nwin);
+        uint32_t cnt = __ldg(a.wcount + w0);
+        bool seen = (w0 == 0);
         AT carry = (AT)0;
-        uint32_t W = TILED ? (P0 / ths) * ths : (P0 / V) * V;
-        for (; W < P1; W += WS) {
-            const uint32_t qb = W + (uint32_t)lane * V;
-            // ---- pass A: the row of each of the lane's positions, real or padding
-            int ridx[VMAX];
-            bool real[VMAX];
-            bool anyreal = false;
-            int cur = -1;
-            if (qb + V > P0 && qb < P1) {
-                const uint32_t qf = max(qb, P0);
-                int lo = 0, hi = nr - 1;
-                while (lo < hi) {
-                    int mid = (lo + hi + 1) >> 1;
-                    if (rps[mid] <= qf) lo = mid; else hi = mid - 1;
-                }
-                cur = lo;
-            }
-#pragma unroll
-            for (int k = 0; k < VMAX; k++) {
-                const uint32_t q = qb + k;
-                ridx[k] = -1;
-                real[k] = false;
-                if (k < (int)V && cur >= 0 && q >= P0 && q < P1) {
-                    while (cur + 1 < nr && rps[cur + 1] <= q) cur++;
-                    ridx[k] = cur;
-                    real[k] = q < rre[cur];
-                    anyreal |= real[k];
+        for (uint32_t w = w0; w < a.nwin; w++) {
+            const bool over = w >= w1;
+            if (over && !seen) break;
+            const uint32_t qb = w * WS + (uint32_t)lane * V;
+            const bool inb = qb < a.npos;  // rows end on V boundaries: whole lanes only
+            const bool st = inb && ((__ldg(a.sbits + (qb >> 5)) >> (qb & 31)) & 1u);
+            const unsigned smask = __ballot_sync(kFull, st);
+            unsigned vl = __ballot_sync(kFull, inb);
+            if (!seen || over) {
+                if (smask == 0u) {
+                    if (!seen) continue;  // all of it continues an earlier warp's row
+                } else {
+                    const unsigned before = (1u << (__ffs(smask) - 1)) - 1u;
+                    vl = seen ? (vl & before) : (vl & ~before);
                 }
             }
-            // ---- loads, gathers, products
-            PT prod[VMAX];
+            const bool valid = (vl >> lane) & 1u;
+            uint32_t rb = valid ? FULLV : 0u;
+            if constexpr (PADDED) rb &= get_bits(a.rbits, qb, V);
+            // ---- the lane's partial sum (loads and gathers of real positions only)
+            AT acc = (AT)0;
+            if (rb) {
+                PT p[V];
+                if constexpr (BAKED) {
 #pragma unroll
-            for (int k = 0; k < VMAX; k++) prod[k] = (PT)0;
-            if constexpr (BAKED) {
-#pragma unroll
-                for (int k = 0; k < VMAX; k++) {
-                    if (real[k]) {
-                        uint32_t q = qb + k, s;
-                        if constexpr (TILED) {
-                            uint32_t t = q / ths, rem = q - t * ths, c = rem / a.th;
-                            s = t * ths + (rem - c * a.th) * a.thw + c;
-                        } else {
-                            s = q;
+                    for (int k = 0; k < V; k++) {
+                        p[k] = (PT)0;
+                        if ((rb >> k) & 1u) {
+                            uint32_t s = qb + k;
+                            if constexpr (TILED) {
+                                const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
+                                s = t * ths + (uint32_t)k * a.thw + c;
+                            }
+                            const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                            p[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
                         }
-                        uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
-                        prod[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
                     }
-                }
-            } else if constexpr (!TILED) {
-                if (anyreal) {
-                    VT v[VMAX];
-                    IT c[VMAX];
-                    if (qb + VMAX <= a.nslots) {
-                        VecLoad<VT, VMAX>::run(val + qb, v);
-                        VecLoad<IT, VMAX>::run(col + qb, c);
-                    } else {  // stream tail: element loads, never past the last slot
+                } else {
+                    VT v[V];
+                    IT c[V];
+                    if constexpr (TILED) {
+                        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
+                        const uint32_t s0 = t * ths + cc;
 #pragma unroll
-                        for (int k = 0; k < VMAX; k++) {
-                            if (real[k]) {
+                        for (int k = 0; k < V; k++) {
+                            v[k] = (VT)0;
+                            c[k] = 0;
+                            if ((rb >> k) & 1u) {
+                                v[k] = ld_stream(val + s0 + (uint32_t)k * a.thw);
+                                c[k] = ld_stream(col + s0 + (uint32_t)k * a.thw);
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < V; k++) {
+                            v[k] = (VT)0;
+                            c[k] = 0;
+                            if ((rb >> k) & 1u) {
                                 v[k] = ld_stream(val + qb + k);
                                 c[k] = ld_stream(col + qb + k);
                             }
                         }
                     }
-                    XT xv[VMAX];
+                    const uint32_t cbase = (sizeof(IT) == 2) ? __ldg(a.colbase + w) : 0u;
+                    XT xv[V];
 #pragma unroll
-                    for (int k = 0; k < VMAX; k++)
-                        xv[k] = real[k] ? __ldg(x + (cbase + (uint32_t)c[k])) : (XT)0;
+                    for (int k = 0; k < V; k++)
+                        xv[k] = ((rb >> k) & 1u) ? __ldg(x + (cbase + (uint32_t)c[k])) : (XT)0;
 #pragma unroll
-                    for (int k = 0; k < VMAX; k++)
-                        if (real[k])
-                            prod[k] = mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k]);
+                    for (int k = 0; k < V; k++)
+                        p[k] = ((rb >> k) & 1u)
+                                   ? mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k])
+                                   : (PT)0;
                 }
-            } else {
-                VT v[VMAX];
-                IT c[VMAX];
 #pragma unroll
-                for (int k = 0; k < VMAX; k++) {
-                    if (real[k]) {
-                        uint32_t q = qb + k;
-                        uint32_t t = q / ths, rem = q - t * ths, cc = rem / a.th;
-                        uint32_t s = t * ths + (rem - cc * a.th) * a.thw + cc;
-                        v[k] = ld_stream(val + s);
-                        c[k] = ld_stream(col + s);
-                    }
-                }
-                XT xv[VMAX];
-#pragma unroll
-                for (int k = 0; k < VMAX; k++)
-                    xv[k] = real[k] ? __ldg(x + (cbase + (uint32_t)c[k])) : (XT)0;
-#pragma unroll
-                for (int k = 0; k < VMAX; k++)
-                    if (real[k]) prod[k] = mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k]);
+                for (int k = 0; k < V; k++) acc = add_rn(acc, (AT)p[k]);
             }
-            // ---- pass B: sequential lane sum with row breaks
-            int first = -1, last = -1, nb = 0;
-            bool starts = false;
-            AT head = (AT)0, acc = (AT)0;
-            uint32_t qlast = 0;
-#pragma unroll
-            for (int k = 0; k < VMAX; k++) {
-                if (ridx[k] < 0) continue;
-                const uint32_t q = qb + k;
-                if (first < 0) {
-                    first = last = ridx[k];
-                    starts = (q == rps[first]);
-                } else if (ridx[k] != last) {
-                    if (nb == 0) head = acc;
-                    else store_y<YT, AT>(y + R0 + last, acc);  // row entirely in this lane
-                    nb++;
-                    acc = (AT)0;
-                    last = ridx[k];
-                }
-                if (real[k]) acc = add_rn(acc, (AT)prod[k]);
-                qlast = q;
-            }
-            const bool has = first >= 0;
-            const bool ends = has && (qlast + 1 == rps[last + 1]);
-            // ---- segmented inclusive scan of the lanes' last segments
-            const bool rf = has && (nb > 0 || starts);
-            const unsigned rmask = __ballot_sync(kFull, rf);
-            const unsigned le = rmask & (kFull >> (31 - lane));
+            // ---- join the lanes of each row, write the rows that end in this window
+            const unsigned sm = smask & vl;
+            const unsigned le = sm & mine;
             const int sstart = le ? 31 - __clz(le) : -1;
             AT S = acc;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
-                AT t = shfl_up(S, d);
+                AT t = __shfl_up_sync(kFull, S, d);
                 if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
             }
             if (sstart < 0) S = add_rn(S, carry);
-            AT E = shfl_up(S, 1);
-            if (lane == 0) E = carry;
-            if (has) {
-                if (nb > 0) store_y<YT, AT>(y + R0 + first, starts ? head : add_rn(head, E));
-                if (ends) store_y<YT, AT>(y + R0 + last, S);
+            bool nxt;
+            if (lane < 31) nxt = (smask >> (lane + 1)) & 1u;
+            else nxt = (qb + V < a.npos) ? ((__ldg(a.sbits + ((qb + V) >> 5)) >> ((qb + V) & 31)) & 1u)
+                                         : true;
+            if (qb + V >= a.npos) nxt = true;
+            if (valid && nxt) {
+                const uint32_t rank = cnt + (uint32_t)__popc(le) - 1u;
+                store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + rank) : rank), S);
             }
-            carry = shfl_idx(S, 31);
+            carry = __shfl_sync(kFull, S, 31);
+            cnt += (uint32_t)__popc(sm);
+            seen = true;
+            if (over && smask != 0u) break;  // the range's last row ended in this window
         }
     }
 }
 
-template <class VT, class IT, class XT, class PT, class AT, class YT, int VMAX, bool TILED,
-          bool BAKED>
-gs_status launch_rpu(const RowsArgs &a, uint32_t rpu, cudaStream_t s)
+// ---------------------------------------------------------------------------------------
+// Striped kernel for the direct (tileH = 1) layouts: lane L takes position 32c + L of each
+// 32-position chunk c, so every load instruction of the warp is one contiguous 256 B
+// (values) / 128 B (columns) access and the chunk's row structure is a single broadcast
+// word of the start bitmap.  Each step handles SU chunks: all their stream loads, then all
+// their x gathers, then the per-chunk segmented scans -- many independent requests per
+// warp, few registers, full occupancy.  Ranges are whole windows of the plan (32*V
+// positions) so the plan's per-window start counts give each range its first row rank.
+constexpr int kStripeU = 4;
+
+// One chunk after its loads and gathers: ownership masks, segmented scan of the lanes'
+// products, y writes of the rows that end in the chunk, carry.  Returns false once the
+// warp's last row has ended past its range ("over").
+template <class AT, class YT, class PT, bool EMPTY>
+__device__ __forceinline__ bool stripe_chunk(const RowsArgs &a, YT *y, int lane, unsigned lt,
+                                             uint32_t ch, uint32_t nchunk, bool over,
+                                             uint32_t word, uint32_t vm, PT prod, uint32_t &cnt,
+                                             bool &seen, AT &carry)
 {
-    uint32_t nunits = (a.nrows + rpu - 1) / rpu;
-    if (nunits == 0) return GS_OK;
-    uint32_t blocks = (nunits + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    blocks = min(blocks, 148u * 64u);
-    switch (rpu) {
-    case 32:
-        k_rows<VT, IT, XT, PT, AT, YT, VMAX, TILED, BAKED, 32>
-            <<<blocks, kWarpsPerBlock * 32, 0, s>>>(a, nunits);
-        break;
-    case 64:
-        k_rows<VT, IT, XT, PT, AT, YT, VMAX, TILED, BAKED, 64>
-            <<<blocks, kWarpsPerBlock * 32, 0, s>>>(a, nunits);
-        break;
-    case 128:
-        k_rows<VT, IT, XT, PT, AT, YT, VMAX, TILED, BAKED, 128>
-            <<<blocks, kWarpsPerBlock * 32, 0, s>>>(a, nunits);
-        break;
-    default: return fail(GS_ERR_UNSUPPORTED, "rows per unit %u not supported", rpu);
+    uint32_t vmw = vm;
+    const uint32_t sw0 = word & vmw;
+    if (!seen || over) {
+        if (sw0 == 0u) {
+            if (!seen) return !over;  // all of it continues an earlier warp's row
+        } else {
+            const uint32_t below = (1u << (__ffs(sw0) - 1)) - 1u;
+            vmw = seen ? (vmw & below) : (vmw & ~below);
+        }
     }
+    const uint32_t sw = word & vmw;
+    const unsigned mine = lt | (1u << lane);
+    const bool valid = (vmw >> lane) & 1u;
+    const unsigned le = sw & mine;
+    const int sstart = le ? 31 - __clz(le) : -1;
+    AT S = valid ? (AT)prod : (AT)0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        AT t = __shfl_up_sync(kFull, S, d);
+        if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
+    }
+    if (sstart < 0) S = add_rn(S, carry);
+    // does the row in progress at this lane end here?
+    bool nxt;
+    if (lane < 31) nxt = (word >> (lane + 1)) & 1u;
+    else nxt = (ch + 1 < nchunk) ? (__ldg(a.sbits + ch + 1) & 1u) : true;
+    if (ch * 32u + (uint32_t)lane + 1u >= a.npos) nxt = true;
+    if (valid && nxt) {
+        const uint32_t rank = cnt + (uint32_t)__popc(sw & mine) - 1u;
+        store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + rank) : rank), S);
+    }
+    carry = __shfl_sync(kFull, S, 31);
+    cnt += (uint32_t)__popc(sw);
+    seen = true;
+    return !(over && sw0 != 0u);
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, bool BAKED, bool PADDED,
+          bool EMPTY>
+__global__ void __launch_bounds__(256) k_rows_striped(const RowsArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    YT *y = static_cast<YT *>(a.y);
+    const VT *val = static_cast<const VT *>(a.val);
+    const IT *col = static_cast<const IT *>(a.col);
+    const XT *x = static_cast<const XT *>(a.x);
+    const double *ax = static_cast<const double *>(a.val);
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t cpwin = a.V;  // chunks per plan window
+    const unsigned lt = (1u << lane) - 1u;  // lanes below this one
+
+    if constexpr (EMPTY) {
+        for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
+            store_y<YT, AT>(y + __ldg(a.empty + i), (AT)0);
+    }
+    const uint32_t nchunk = (a.npos + 31) / 32;
+    // stream loads of chunk ch for this lane: start-bit word, in-bounds mask, real mask
+    auto load_chunk = [&](uint32_t ch, uint32_t lim, uint32_t &word, uint32_t &vm,
+                          uint32_t &rm, VT &v, IT &c, double &xb) {
+        const uint32_t q = ch * 32u + (uint32_t)lane;
+        const bool in = ch < lim;
+        word = in ? __ldg(a.sbits + ch) : 0u;
+        vm = !in ? 0u
+             : (ch * 32u + 32u <= a.npos ? 0xffffffffu : ((1u << (a.npos - ch * 32u)) - 1u));
+        rm = (PADDED ? (in ? __ldg(a.rbits + ch) : 0u) : 0xffffffffu) & vm;
+        v = (VT)0;
+        c = 0;
+        xb = 0.0;
+        if ((rm >> lane) & 1u) {
+            if constexpr (BAKED) {
+                const uint32_t ai = (q / a.axw) * 2u * a.axw + q % a.axw;
+                v = __ldcs(ax + ai);
+                xb = __ldcs(ax + ai + a.axw);
+            } else {
+                v = ld_stream(val + q);
+                c = ld_stream(col + q);
+            }
+        }
+    };
+    // x gather and product of the lane's position (0 when not real)
+    auto product = [&](uint32_t ch, uint32_t rm, VT v, IT c, double xb) -> PT {
+        if (!((rm >> lane) & 1u)) return (PT)0;
+        if constexpr (BAKED) {
+            return (PT)mul_rn(v, xb);
+        } else {
+            const uint32_t cbase = (sizeof(IT) == 2) ? __ldg(a.colbase + ch / cpwin) : 0u;
+            return mul_rn((PT)ValTraits<VT>::to_f64(v), (PT)__ldg(x + (cbase + (uint32_t)c)));
+        }
+    };
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    for (uint32_t rg = gw; rg < nranges; rg += nwarps) {
+        const uint32_t c0 = rg * a.wpw * cpwin;
+        const uint32_t c1 = min(c0 + a.wpw * cpwin, nchunk);
+        uint32_t cnt = __ldg(a.wcount + rg * a.wpw);  // row starts before the range
+        bool seen = (c0 == 0);
+        AT carry = (AT)0;
+        // the range's own chunks, kStripeU at a time: all loads, then all gathers, then the
+        // per-chunk scans
+        for (uint32_t cb = c0; cb < c1; cb += kStripeU) {
+            uint32_t word[kStripeU], vm[kStripeU], rm[kStripeU];
+            VT v[kStripeU];
+            IT c[kStripeU];
+            double xb[kStripeU];
+            PT prod[kStripeU];
+#pragma unroll
+            for (int u = 0; u < kStripeU; u++)
+                load_chunk(cb + u, c1, word[u], vm[u], rm[u], v[u], c[u], xb[u]);
+#pragma unroll
+            for (int u = 0; u < kStripeU; u++) prod[u] = product(cb + u, rm[u], v[u], c[u], xb[u]);
+#pragma unroll
+            for (int u = 0; u < kStripeU; u++)
+                if (cb + u < c1)
+                    stripe_chunk<AT, YT, PT, EMPTY>(a, y, lane, lt, cb + u, nchunk, false,
+                                                    word[u], vm[u], prod[u], cnt, seen, carry);
+        }
+        // past the range: one chunk at a time until the range's last row ends
+        if (seen) {
+            for (uint32_t ch = c1; ch < nchunk; ch++) {
+                uint32_t word, vm, rm;
+                VT v;
+                IT c;
+                double xb;
+                load_chunk(ch, nchunk, word, vm, rm, v, c, xb);
+                const PT p = product(ch, rm, v, c, xb);
+                if (!stripe_chunk<AT, YT, PT, EMPTY>(a, y, lane, lt, ch, nchunk, true, word, vm,
+                                                     p, cnt, seen, carry))
+                    break;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// TMA-staged kernel for tiled layouts with 32-wide tiles (tileHW = 32, tileH = TH): a window
+// is exactly one tile.  Each warp owns a contiguous range of tiles and keeps kTmaStages of
+// them in flight in its shared-memory ring; stage layout: [val tile | col tile | start
+// bits | real bits] (baked: [ax tile | start bits | real bits]).
+template <class VT, class IT, int TH, bool BAKED, bool PADDED>
+struct TmaStage {
+    static constexpr uint32_t WS = 32u * TH;
+    static constexpr uint32_t VAL = BAKED ? 2u * WS * 8u : WS * (uint32_t)sizeof(VT);
+    static constexpr uint32_t COL = BAKED ? 0u : WS * (uint32_t)sizeof(IT);
+    static constexpr uint32_t BITS = (uint32_t)TH * 4u;
+    static constexpr uint32_t COPY = VAL + COL + BITS * (PADDED ? 2u : 1u);
+    static constexpr uint32_t BYTES = (COPY + 127u) & ~127u;
+    static constexpr uint32_t PER_WARP = BYTES * kTmaStages;
+    static constexpr uint32_t SMEM = PER_WARP * kTmaWarps + kTmaWarps * kTmaStages * 8u;
+};
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int TH, bool BAKED,
+          bool PADDED, bool EMPTY>
+__global__ void __launch_bounds__(kTmaWarps * 32) k_rows_tma(const RowsArgs a)
+{
+    using ST = TmaStage<VT, IT, TH, BAKED, PADDED>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    unsigned char *ring = smem + wib * ST::PER_WARP;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kTmaWarps * ST::PER_WARP) +
+                     wib * kTmaStages;
+    YT *y = static_cast<YT *>(a.y);
+    const XT *x = static_cast<const XT *>(a.x);
+    constexpr uint32_t V = TH;
+    constexpr uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
+    constexpr uint32_t WS = ST::WS;
+    const uint32_t nwarps = gridDim.x * kTmaWarps;
+    const uint32_t gw = blockIdx.x * kTmaWarps + wib;
+
+    if constexpr (EMPTY) {
+        for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
+            store_y<YT, AT>(y + __ldg(a.empty + i), (AT)0);
+    }
+    // contiguous, equal ranges of tiles (positions) per warp
+    const uint32_t per = (a.nwin + nwarps - 1) / nwarps;
+    const uint32_t w0 = gw * per;
+    const uint32_t w1 = min(w0 + per, a.nwin);
+    if (w0 >= w1) return;
+
+    if (lane == 0) {
+        for (int s = 0; s < kTmaStages; s++) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    auto issue = [&](uint32_t w, int s) {
+        if (lane == 0) {
+            unsigned char *st = ring + s * ST::BYTES;
+            mbar_expect_tx(&bars[s], ST::COPY);
+            if constexpr (BAKED) {
+                bulk_g2s(st, static_cast<const double *>(a.val) + (size_t)w * 2u * WS, ST::VAL,
+                         &bars[s]);
+            } else {
+                bulk_g2s(st, static_cast<const VT *>(a.val) + (size_t)w * WS, ST::VAL, &bars[s]);
+                bulk_g2s(st + ST::VAL, static_cast<const IT *>(a.col) + (size_t)w * WS, ST::COL,
+                         &bars[s]);
+            }
+            bulk_g2s(st + ST::VAL + ST::COL, a.sbits + (size_t)w * TH, ST::BITS, &bars[s]);
+            if constexpr (PADDED)
+                bulk_g2s(st + ST::VAL + ST::COL + ST::BITS, a.rbits + (size_t)w * TH, ST::BITS,
+                         &bars[s]);
+        }
+    };
+    const uint32_t npre = min((uint32_t)kTmaStages, w1 - w0);
+    for (uint32_t i = 0; i < npre; i++) issue(w0 + i, (int)i);
+
+    uint32_t cnt = __ldg(a.wcount + w0);
+    bool seen = (w0 == 0);
+    AT carry = (AT)0;
+    uint32_t parity = 0;  // bit s: phase parity expected next at stage s
+    for (uint32_t w = w0; w < w1; w++) {
+        const int s = (int)((w - w0) % kTmaStages);
+        if (!mbar_wait_bounded(&bars[s], (parity >> s) & 1u)) {
+            // the copy never completed: report, drain what is in flight (bounded), leave
+            if (lane == 0) atomicOr(a.status, 1u);
+            for (uint32_t v = w; v < min(w + (uint32_t)kTmaStages, w1); v++) {
+                const int t = (int)((v - w0) % kTmaStages);
+                mbar_wait_bounded(&bars[t], (parity >> t) & 1u);
+            }
+            return;
+        }
+        parity ^= 1u << s;
+        const unsigned char *st = ring + s * ST::BYTES;
+        const uint32_t *sbw = reinterpret_cast<const uint32_t *>(st + ST::VAL + ST::COL);
+        const uint32_t W = w * WS;
+        const uint32_t lb = (uint32_t)lane * V;
+        const uint32_t sraw = (sbw[lb >> 5] >> (lb & 31)) & FULLV;
+        const WinCtl ctl = window_ctl(lane, W, V, FULLV, a.npos, sraw, seen, false);
+        if (!ctl.skip) {
+            uint32_t rb = ctl.vmask;
+            if constexpr (PADDED) rb &= (sbw[TH + (lb >> 5)] >> (lb & 31));
+            PT prod[TH];
+            if constexpr (BAKED) {
+                const double *sax = reinterpret_cast<const double *>(st);
+#pragma unroll
+                for (int k = 0; k < TH; k++)
+                    prod[k] = ((rb >> k) & 1u)
+                                  ? (PT)mul_rn(sax[2 * 32 * k + lane], sax[2 * 32 * k + 32 + lane])
+                                  : (PT)0;
+            } else {
+                const VT *sv = reinterpret_cast<const VT *>(st);
+                const IT *sc = reinterpret_cast<const IT *>(st + ST::VAL);
+                XT xv[TH];
+#pragma unroll
+                for (int k = 0; k < TH; k++)
+                    xv[k] = ((rb >> k) & 1u) ? __ldg(x + (uint32_t)sc[32 * k + lane]) : (XT)0;
+#pragma unroll
+                for (int k = 0; k < TH; k++)
+                    prod[k] = ((rb >> k) & 1u)
+                                  ? mul_rn((PT)ValTraits<VT>::to_f64(sv[32 * k + lane]), (PT)xv[k])
+                                  : (PT)0;
+            }
+            window_reduce<AT, YT, TH, EMPTY, PT>(a, y, lane, W, V, sraw, ctl.vmask, rb, prod,
+                                                 cnt, carry);
+            seen = true;
+        }
+        __syncwarp();
+        if (w + kTmaStages < w1) {
+            fence_proxy_async();  // our reads of this stage precede the next bulk write to it
+            issue(w + kTmaStages, s);
+        }
+    }
+    if (seen)
+        finish_overhang<VT, IT, XT, PT, AT, YT, TH, true, BAKED, PADDED, EMPTY>(
+            a, y, lane, w1, V, FULLV, cnt, carry);
+}
+
+// ---------------------------------------------------------------------------------------
+template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
+          bool BAKED>
+gs_status launch_k(const RowsArgs &a, bool padded, cudaStream_t s)
+{
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    uint32_t warps = nranges;
+    if (a.n_empty) warps = max(warps, min((a.n_empty + 31) / 32, 148u * 64u));
+    if (warps == 0) return GS_OK;
+    uint32_t blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    blocks = min(blocks, 148u * 256u);
+    const bool empty = a.n_empty != 0;
+#define GS_L(P, E)                                                                          \
+    k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
+    if (padded) {
+        if (empty) GS_L(true, true); else GS_L(true, false);
+    } else {
+        if (empty) GS_L(false, true); else GS_L(false, false);
+    }
+#undef GS_L
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
+          bool BAKED>
+gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
+{
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    uint32_t warps = nranges;
+    if (a.n_empty) warps = max(warps, min((a.n_empty + 31) / 32, 148u * 64u));
+    if (warps == 0) return GS_OK;
+    uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
+    const bool empty = a.n_empty != 0;
+#define GS_L(P, E)                                                                          \
+    k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E><<<blocks, 256, 0, s>>>(a)
+    if (padded) {
+        if (empty) GS_L(true, true); else GS_L(true, false);
+    } else {
+        if (empty) GS_L(false, true); else GS_L(false, false);
+    }
+#undef GS_L
     GS_CHECK_LAUNCH();
     return GS_OK;
 }
 
 template <class VT, class IT, class XT, class PT, class AT, class YT, bool BAKED>
-gs_status launch_shape(const RowsArgs &a, bool tiled, uint32_t lane_pos, uint32_t rpu,
+gs_status launch_striped(const RowsArgs &a, bool padded, cudaStream_t s)
+{
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    uint32_t warps = nranges;
+    if (a.n_empty) warps = max(warps, min((a.n_empty + 31) / 32, 148u * 64u));
+    if (warps == 0) return GS_OK;
+    uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
+    const bool empty = a.n_empty != 0;
+#define GS_L(P, E) k_rows_striped<VT, IT, XT, PT, AT, YT, BAKED, P, E><<<blocks, 256, 0, s>>>(a)
+    if (padded) {
+        if (empty) GS_L(true, true); else GS_L(true, false);
+    } else {
+        if (empty) GS_L(false, true); else GS_L(false, false);
+    }
+#undef GS_L
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int TH, bool BAKED,
+          bool PADDED, bool EMPTY>
+gs_status launch_tma_one(const RowsArgs &a, cudaStream_t s)
+{
+    using ST = TmaStage<VT, IT, TH, BAKED, PADDED>;
+    auto kern = k_rows_tma<VT, IT, XT, PT, AT, YT, TH, BAKED, PADDED, EMPTY>;
+    static int blocks_per_sm = -1;  // per instantiation, resolved on first launch
+    static int sms = 0;
+    if (blocks_per_sm < 0) {
+        GS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ST::SMEM));
+        int dev = 0;
+        GS_CUDA(cudaGetDevice(&dev));
+        GS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        int bps = 0;
+        GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kTmaWarps * 32,
+                                                              ST::SMEM));
+        blocks_per_sm = bps > 0 ? bps : 1;
+    }
+    uint32_t blocks = (uint32_t)(blocks_per_sm * sms);
+    const uint32_t need = (a.nwin + kTmaWarps - 1) / kTmaWarps;
+    if (need < blocks) blocks = max(need, 1u);
+    kern<<<blocks, kTmaWarps * 32, ST::SMEM, s>>>(a);
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int TH, bool BAKED>
+gs_status launch_tma(const RowsArgs &a, bool padded, cudaStream_t s)
+{
+    const bool empty = a.n_empty != 0;
+    if (padded) {
+        if (empty) return launch_tma_one<VT, IT, XT, PT, AT, YT, TH, BAKED, true, true>(a, s);
+        return launch_tma_one<VT, IT, XT, PT, AT, YT, TH, BAKED, true, false>(a, s);
+    }
+    if (empty) return launch_tma_one<VT, IT, XT, PT, AT, YT, TH, BAKED, false, true>(a, s);
+    return launch_tma_one<VT, IT, XT, PT, AT, YT, TH, BAKED, false, false>(a, s);
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, bool BAKED>
+gs_status launch_shape(const RowsArgs &a, bool tiled, bool padded, uint32_t flags,
                        cudaStream_t s)
 {
+    const bool tma = (flags & GS_FLAG_TMA) != 0;
+    const bool striped = (flags & GS_FLAG_STRIPED) != 0;
     if constexpr (!std::is_same<VT, double>::value) {
-        // reduced-precision storage: direct (tileH = 1) layouts, 8 positions per lane
-        (void)lane_pos;
-        if (tiled)
-            return fail(GS_ERR_UNSUPPORTED, "FP32/BF16 storage needs a tileH=1 layout");
-        return launch_rpu<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, rpu, s);
+        if (tiled) return fail(GS_ERR_UNSUPPORTED, "FP32/BF16 storage needs a tileH=1 layout");
+        if (a.aligned && a.V == 8)
+            return launch_aligned<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, padded, s);
+        if (a.V != kDirectV) return fail(GS_ERR_INVALID, "plan built for another shape");
+        if (striped) return launch_striped<VT, IT, XT, PT, AT, YT, BAKED>(a, padded, s);
+        return launch_k<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, padded, s);
     } else {
         if (tiled) {
-            if (a.th <= 4) return launch_rpu<VT, IT, XT, PT, AT, YT, 4, true, BAKED>(a, rpu, s);
-            if (a.th <= 8) return launch_rpu<VT, IT, XT, PT, AT, YT, 8, true, BAKED>(a, rpu, s);
+            if (tma && a.thw == 32 && a.status) {
+                if (a.th == 4) return launch_tma<VT, IT, XT, PT, AT, YT, 4, BAKED>(a, padded, s);
+                if (a.th == 8) return launch_tma<VT, IT, XT, PT, AT, YT, 8, BAKED>(a, padded, s);
+                if (a.th == 16)
+                    return launch_tma<VT, IT, XT, PT, AT, YT, 16, BAKED>(a, padded, s);
+            }
+            if (a.aligned) {
+                switch (a.th) {
+                case 2: return launch_aligned<VT, IT, XT, PT, AT, YT, 2, true, BAKED>(a, padded, s);
+                case 4: return launch_aligned<VT, IT, XT, PT, AT, YT, 4, true, BAKED>(a, padded, s);
+                case 8: return launch_aligned<VT, IT, XT, PT, AT, YT, 8, true, BAKED>(a, padded, s);
+                case 16:
+                    return launch_aligned<VT, IT, XT, PT, AT, YT, 16, true, BAKED>(a, padded, s);
+                default: break;
+                }
+            }
+            if (a.th <= 4) return launch_k<VT, IT, XT, PT, AT, YT, 4, true, BAKED>(a, padded, s);
+            if (a.th <= 8) return launch_k<VT, IT, XT, PT, AT, YT, 8, true, BAKED>(a, padded, s);
             if (a.th <= 16)
-                return launch_rpu<VT, IT, XT, PT, AT, YT, 16, true, BAKED>(a, rpu, s);
+                return launch_k<VT, IT, XT, PT, AT, YT, 16, true, BAKED>(a, padded, s);
             return fail(GS_ERR_UNSUPPORTED, "tileH %u > 16 not supported by the kernels", a.th);
         }
-        if (lane_pos == 8) return launch_rpu<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, rpu, s);
-        return launch_rpu<VT, IT, XT, PT, AT, YT, 4, false, BAKED>(a, rpu, s);
+        if (a.aligned) {
+            switch (a.V) {
+            case 4: return launch_aligned<VT, IT, XT, PT, AT, YT, 4, false, BAKED>(a, padded, s);
+            case 8: return launch_aligned<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, padded, s);
+            case 16: return launch_aligned<VT, IT, XT, PT, AT, YT, 16, false, BAKED>(a, padded, s);
+            default: break;
+            }
+        }
+        if (a.V != kDirectV) return fail(GS_ERR_INVALID, "plan built for another shape");
+        if (striped) return launch_striped<VT, IT, XT, PT, AT, YT, BAKED>(a, padded, s);
+        return launch_k<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, padded, s);
+    }
+}
+
+// ------------------------------------------------------------------ plan construction
+__global__ void k_set_starts(uint32_t n, const uint32_t *rpos, uint32_t *sbits)
+{
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n && rpos[r + 1] > rpos[r]) atomicOr(sbits + (rpos[r] >> 5), 1u << (rpos[r] & 31));
+}
+
+__global__ void k_set_real(uint32_t n, const uint32_t *rpos, const uint32_t *rlen,
+                           uint32_t *rbits)
+{
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    uint32_t p = rpos[r];
+    const uint32_t e = p + rlen[r];
+    while (p < e) {
+        const uint32_t w = p >> 5, b = p & 31;
+        const uint32_t cnt = min(32u - b, e - p);
+        const uint32_t m = (cnt == 32 ? 0xffffffffu : ((1u << cnt) - 1u)) << b;
+        atomicOr(rbits + w, m);
+        p += cnt;
+    }
+}
+
+__global__ void k_narrow_u32(uint32_t n1, const uint64_t *a, uint32_t *b)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n1) b[i] = (uint32_t)a[i];
+}
+
+__global__ void k_split_rows(uint32_t n, const uint32_t *rpos, const uint64_t *pre,
+                             uint32_t *ne, uint32_t *empty)
+{
+    uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t k = (uint32_t)pre[r];
+    if (rpos[r + 1] > rpos[r]) ne[k] = r;
+    else empty[r - k] = r;
+}
+
+// per window: min column over real positions -> base; flag if the spread exceeds 16 bits;
+// then col16 = col32 - base (padding slots keep 0)
+__global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, const uint32_t *col32,
+                           const uint32_t *rbits, uint32_t *colbase, uint16_t *col16,
+                           uint32_t *flag)
+{
+    const int lane = threadIdx.x & 31;
+    for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nwin;
+         w += gridDim.x * (blockDim.x >> 5)) {
+        const uint32_t b = w * WS, e = min(b + WS, nslots);
+        uint32_t mn = 0xffffffffu, mx = 0;
+        for (uint32_t s = b + lane; s < e; s += 32) {
+            const bool real = !rbits || ((rbits[s >> 5] >> (s & 31)) & 1u);
+            if (real) { mn = min(mn, col32[s]); mx = max(mx, col32[s]); }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = min(mn, __shfl_xor_sync(kFull, mn, o));
+            mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+        }
+        const uint32_t base = (mn == 0xffffffffu) ? 0u : mn;
+        if (lane == 0) {
+            colbase[w] = base;
+            if (mn != 0xffffffffu && mx - mn > 65535u) atomicOr(flag, 1u);
+        }
+        for (uint32_t s = b + lane; s < e; s += 32) {
+            const bool real = !rbits || ((rbits[s >> 5] >> (s & 31)) & 1u);
+            col16[s] = real ? (uint16_t)(col32[s] - base) : (uint16_t)0;
+        }
     }
 }
 
 }  // namespace
 
-uint32_t choose_rpu(uint32_t nrows, uint64_t positions, uint32_t lane_pos)
+gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
+                          uint32_t V, RowsPlan &P, cudaStream_t s)
 {
-    // aim for at least ~4 windows of work per warp unit
-    double avg = nrows ? (double)positions / nrows : 0.0;
-    double target = 4.0 * 32.0 * lane_pos;
-    if (avg * 32 >= target) return 32;
-    if (avg * 64 >= target) return 64;
-    return 128;
+    P.V = V;
+    P.padded = d_rlen != nullptr;
+    uint32_t npos = 0;
+    GS_CUDA(cudaMemcpyAsync(&npos, d_rpos + n, 4, cudaMemcpyDeviceToHost, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    P.npos = npos;
+    const uint64_t WS = 32ull * V;
+    P.nwin = (uint32_t)(((uint64_t)npos + WS - 1) / WS);
+    // windows per warp range of the LDG kernel: ~1024 positions, fewer when the matrix is
+    // too small to give every SM enough warps
+    uint32_t wpw = (uint32_t)((1024 + WS - 1) / WS);
+    while (wpw > 1 && (uint64_t)P.nwin / wpw < 148ull * 48ull) wpw >>= 1;
+    P.wpw = wpw;
+    const size_t words = (size_t)P.nwin * V + 2;
+    GS_TRY(P.sbits.alloc_zero(words * 4, s));
+    const unsigned g = (n + 255) / 256;
+    k_set_starts<<<g, 256, 0, s>>>(n, d_rpos, P.sbits.as<uint32_t>());
+    GS_CHECK_LAUNCH();
+    if (P.padded) {
+        GS_TRY(P.rbits.alloc_zero(words * 4, s));
+        k_set_real<<<g, 256, 0, s>>>(n, d_rpos, d_rlen, P.rbits.as<uint32_t>());
+        GS_CHECK_LAUNCH();
+    }
+    DevBuf pre;
+    GS_TRY(pre.alloc(((size_t)P.nwin + 1) * 8));
+    CountSpec cw{CountKind::WindowPopc};
+    cw.arr = P.sbits.as<uint32_t>();
+    cw.a = V;
+    GS_TRY(exclusive_scan(cw, P.nwin, pre.as<uint64_t>(), nullptr, s));
+    GS_TRY(P.wcount.alloc(((size_t)P.nwin + 1) * 4));
+    k_narrow_u32<<<(P.nwin + 256) / 256, 256, 0, s>>>(P.nwin + 1, pre.as<uint64_t>(),
+                                                       P.wcount.as<uint32_t>());
+    GS_CHECK_LAUNCH();
+    // empty rows: rank -> row map and the list of rows to zero
+    DevBuf pe;
+    GS_TRY(pe.alloc(((size_t)n + 1) * 8));
+    CountSpec ce{CountKind::NonEmpty};
+    ce.row = d_rpos;
+    uint64_t nonempty = 0;
+    GS_TRY(exclusive_scan(ce, n, pe.as<uint64_t>(), &nonempty, s));
+    P.n_empty = (uint32_t)(n - nonempty);
+    if (P.n_empty) {
+        GS_TRY(P.ne.alloc((size_t)nonempty * 4 + 4));
+        GS_TRY(P.empty.alloc((size_t)P.n_empty * 4));
+        k_split_rows<<<g, 256, 0, s>>>(n, d_rpos, pe.as<uint64_t>(), P.ne.as<uint32_t>(),
+                                       P.empty.as<uint32_t>());
+        GS_CHECK_LAUNCH();
+    }
+    GS_TRY(P.status.alloc_zero(4, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    return GS_OK;
+}
+
+gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &P,
+                            uint16_t *d_col16, cudaStream_t s)
+{
+    GS_TRY(P.colbase.alloc((size_t)P.nwin * 4 + 4));
+    DevBuf flag;
+    GS_TRY(flag.alloc_zero(4, s));
+    const uint32_t blocks = min((P.nwin + 7) / 8, 148u * 64u);
+    if (blocks)
+        k_u16_cols<<<blocks, 256, 0, s>>>(P.nwin, 32u * P.V, nslots, d_col32,
+                                          P.padded ? P.rbits.as<uint32_t>() : nullptr,
+                                          P.colbase.as<uint32_t>(), d_col16, flag.as<uint32_t>());
+    GS_CHECK_LAUNCH();
+    uint32_t hf = 0;
+    GS_CUDA(cudaMemcpyAsync(&hf, flag.p, 4, cudaMemcpyDeviceToHost, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    if (hf)
+        return fail(GS_ERR_UNSUPPORTED,
+                    "a window of %u positions spans more than 65536 columns: 16-bit column "
+                    "offsets do not fit this matrix", 32u * P.V);
+    return GS_OK;
+}
+
+uint32_t aligned_lane_positions(uint32_t align, bool *aligned)
+{
+    *aligned = false;
+    if (align == 0) return kDirectV;
+    for (uint32_t v : {16u, 8u, 4u, 2u}) {
+        if (v > align || align % v) continue;
+        if (v == 16 && align != 16) continue;  // 16 only for 16-high tiles
+        *aligned = true;
+        return v;
+    }
+    return kDirectV;
+}
+
+RowsArgs rows_args(const RowsPlan &P)
+{
+    RowsArgs a{};
+    a.aligned = P.aligned ? 1u : 0u;
+    a.npos = P.npos;
+    a.nwin = P.nwin;
+    a.wpw = P.wpw;
+    a.V = P.V;
+    a.n_empty = P.n_empty;
+    a.sbits = P.sbits.as<uint32_t>();
+    a.rbits = P.rbits.as<uint32_t>();
+    a.wcount = P.wcount.as<uint32_t>();
+    a.ne = P.ne.as<uint32_t>();
+    a.empty = P.empty.as<uint32_t>();
+    a.colbase = P.colbase.as<uint32_t>();
+    a.status = P.status.as<uint32_t>();
+    a.thw = 1;
+    a.th = 1;
+    return a;
 }
 
 gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
-                      uint32_t flags, bool tiled, bool baked, uint32_t lane_pos, uint32_t rpu,
-                      cudaStream_t s)
+                      uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s)
 {
     if (tiled && (a.thw == 0 || 32 % a.thw != 0))
         return fail(GS_ERR_UNSUPPORTED, "tileH>1 kernels need tileHW dividing 32 (got %u)",
                     a.thw);
+    if (tiled && a.V != a.th) return fail(GS_ERR_INVALID, "tiled plan built for another tileH");
     if (baked) {
         if (vtype != GS_F64 || ytype != GS_F64)
             return fail(GS_ERR_UNSUPPORTED, "baked layouts are FP64 only");
         return launch_shape<double, uint32_t, double, double, double, double, true>(
-            a, tiled, lane_pos, rpu, s);
+            a, tiled, padded, flags, s);
     }
     const bool acc64 = (flags & GS_FLAG_ACC_F64) != 0;
     if (vtype == GS_F64) {
         if (ytype != GS_F64 || itype != GS_IDX_U32)
             return fail(GS_ERR_UNSUPPORTED, "FP64 matrices take FP64 y and 32-bit columns");
         return launch_shape<double, uint32_t, double, double, double, double, false>(
-            a, tiled, lane_pos, rpu, s);
+            a, tiled, padded, flags, s);
     }
-#define GS_MIXED(VT_, IT_)                                                                 \
-    do {                                                                                   \
-        if (acc64 && ytype == GS_F64)                                                      \
-            return launch_shape<VT_, IT_, float, float, double, double, false>(            \
-                a, tiled, lane_pos, rpu, s);                                               \
-        if (acc64)                                                                         \
-            return launch_shape<VT_, IT_, float, float, double, float, false>(             \
-                a, tiled, lane_pos, rpu, s);                                               \
-        if (ytype == GS_F64)                                                               \
-            return launch_shape<VT_, IT_, float, float, float, double, false>(             \
-                a, tiled, lane_pos, rpu, s);                                               \
-        return launch_shape<VT_, IT_, float, float, float, float, false>(a, tiled,         \
-                                                                         lane_pos, rpu, s); \
+#define GS_MIXED(VT_, IT_)                                                                   \
+    do {                                                                                     \
+        if (acc64 && ytype == GS_F64)                                                        \
+            return launch_shape<VT_, IT_, float, float, double, double, false>(a, tiled,     \
+                                                                               padded, flags, s); \
+        if (acc64)                                                                           \
+            return launch_shape<VT_, IT_, float, float, double, float, false>(a, tiled,      \
+                                                                              padded, flags, s); \
+        if (ytype == GS_F64)                                                                 \
+            return launch_shape<VT_, IT_, float, float, float, double, false>(a, tiled,      \
+                                                                              padded, flags, s); \
+        return launch_shape<VT_, IT_, float, float, float, float, false>(a, tiled, padded,   \
+                                                                         flags, s);          \
     } while (0)
     if (vtype == GS_F32 && itype == GS_IDX_U32) GS_MIXED(float, uint32_t);
     if (vtype == GS_F32 && itype == GS_IDX_U16) GS_MIXED(float, uint16_t);

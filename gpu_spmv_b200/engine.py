@@ -84,8 +84,12 @@ class Matrix:
 
     # ---------------------------------------------------------------- products
     def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, acc64: bool = False,
-             out_dtype=None, stream=None) -> torch.Tensor:
-        """y = A x on the device (x: ncols entries; FP64 for FP64 matrices, else FP32)."""
+             out_dtype=None, stream=None, tma: bool = False,
+             striped: bool = False) -> torch.Tensor:
+        """y = A x on the device (x: ncols entries; FP64 for FP64 matrices, else FP32).
+        Kernel variants: tma=True stages 32-wide tileH>1 tiles with TMA bulk copies;
+        striped=True maps one position per lane per 32-position chunk (CSR / COM
+        tileH=1) instead of 8 consecutive positions per lane."""
         xt = torch.float64 if self.vtype == L.GS_F64 else torch.float32
         if x.dtype != xt or not x.is_cuda or not x.is_contiguous():
             raise TypeError(f"x must be a contiguous CUDA {xt} tensor")
@@ -94,10 +98,18 @@ class Matrix:
             y = torch.empty(self.nrows, dtype=ydt, device=x.device)
         ycode = L.GS_F64 if y.dtype == torch.float64 else L.GS_F32
         xcode = L.GS_F64 if xt == torch.float64 else L.GS_F32
-        flags = L.GS_FLAG_ACC_F64 if acc64 else L.GS_FLAG_NONE
+        flags = ((L.GS_FLAG_ACC_F64 if acc64 else 0) | (L.GS_FLAG_TMA if tma else 0) |
+                 (L.GS_FLAG_STRIPED if striped else 0))
         L.check(L.lib().gs_spmv(self._h, x.data_ptr(), xcode, y.data_ptr(), ycode, flags,
                                 stream_handle(stream)), "gs_spmv")
         return y
+
+    def device_status(self, reset: bool = True) -> int:
+        """Status word of the kernels (bit 0: a bounded wait timed out); synchronises."""
+        w = L.UIN()
+        L.check(L.lib().gs_matrix_device_status(self._h, C.byref(w), 1 if reset else 0),
+                "gs_matrix_device_status")
+        return w.value
 
     # ---------------------------------------------------------------- layout readback
     def layout(self) -> dict:

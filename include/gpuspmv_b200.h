@@ -286,6 +286,17 @@ double gs_algorithmic_bytes(UIN nrows, UIN ncols, UIN nnz, UIN k, UIN s_v, UIN s
 /* SpMV flags */
 #define GS_FLAG_NONE 0u
 #define GS_FLAG_ACC_F64 1u /* FP32-stored values: FP32 products, FP64 row reduction */
+#define GS_FLAG_TMA 2u        /* tileH > 1 layouts with tileHW = 32: stage the value/column
+                                 tiles in shared memory with TMA bulk copies instead of
+                                 plain loads (kernel variant, for tuning / comparison) */
+#define GS_FLAG_STRIPED 4u    /* CSR / COM tileH = 1 layouts: one position per lane per
+                                 32-position chunk instead of 8 consecutive positions per
+                                 lane (kernel variant) */
+
+/* Device status word of a matrix's kernels: bit 0 = a bounded wait on a TMA stage timed
+ * out (the kernel gave up and its y is incomplete).  Synchronises the device; `reset`
+ * clears the word. */
+gs_status gs_matrix_device_status(const gs_matrix *A, UIN *word, int reset);
 
 /* y = A x on the device.  x has ncols entries of xtype, y nrows entries of ytype.
  * F64 matrices take F64 x/y; F32/BF16 matrices take F32 x and F32 or F64 y.
@@ -303,7 +314,10 @@ gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dty
  * device arrays back without a CUDA runtime of their own). */
 gs_status gs_copy_to_host(void *h_dst, const void *d_src, size_t bytes);
 
-/* CSR SpMV straight from device CSR arrays (no conversion step): y = A x, FP64. */
+/* CSR SpMV straight from device CSR arrays: y = A x, FP64.  Builds the kernel's row-start
+ * plan on every call and returns when y is complete; for repeated products convert once
+ * with gs_matrix_create(GS_FMT_CSR) and call gs_spmv.  val and col must be 16-byte
+ * aligned. */
 gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
                           const double *d_val, const double *d_x, double *d_y,
                           gs_stream stream);

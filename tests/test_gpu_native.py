@@ -66,6 +66,48 @@ def test_native_layout_and_spmv(port, name, fmt):
     A.close()
 
 
+@pytest.mark.parametrize("name", ["mixed", "row0_empty", "dense_row", "powerlaw_small"])
+@pytest.mark.parametrize("mode,th", [("COM", 4), ("COM", 8), ("COM", 16), ("UNC", 4),
+                                     ("UNC", 8), ("UNC", 16)])
+def test_tma_staging_matches_plain_loads(port, name, mode, th):
+    """32-wide tiled layouts run on the TMA-staged kernel; the plain-load kernel sums in the
+    same order, so the two agree to the last bit, and no bounded wait timed out."""
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(th + len(name))
+    row, col, val = case(name, rng)
+    n = len(row) - 1
+    ncols = _square_ncols(row, col)
+    A = E.Matrix(row, col, val, ncols=ncols, fmt="AXT", mode=mode, tileH=th, tileHW=32)
+    x = torch.from_numpy(rng.uniform(-1, 1, ncols)).cuda()
+    y_tma = A.spmv(x, tma=True).cpu().numpy()
+    y_ldg = A.spmv(x, tma=False).cpu().numpy()
+    assert A.device_status() == 0
+    assert np.array_equal(y_tma, y_ldg)
+    _, mag = port.csr_truth(row, col, val, x.cpu().numpy())
+    assert within_bound(y_tma, port.csr_spmv(row, col, val, x.cpu().numpy()), mag)
+    assert len(y_tma) == n
+
+
+@pytest.mark.parametrize("name", ["mixed", "row0_empty", "dense_row", "laplacian"])
+@pytest.mark.parametrize("fmt", [dict(fmt="CSR"), dict(fmt="AXC", hbs=32),
+                                 dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
+                                 dict(fmt="AXT", mode="COM", tileH=1, tileHW=32)],
+                         ids=["csr", "axc", "unc1hw4", "com1"])
+def test_striped_variant(port, name, fmt):
+    """The striped (one position per lane per chunk) kernel variant meets the same bound."""
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(7 + len(name))
+    row, col, val = case(name, rng)
+    ncols = _square_ncols(row, col)
+    A = E.Matrix(row, col, val, ncols=ncols, **fmt)
+    xh = rng.uniform(-1, 1, ncols)
+    y = A.spmv(torch.from_numpy(xh).cuda(), striped=True).cpu().numpy()
+    _, mag = port.csr_truth(row, col, val, xh)
+    assert within_bound(y, port.csr_spmv(row, col, val, xh), mag)
+
+
 @pytest.mark.parametrize("name", ["mixed", "laplacian", "powerlaw_small"])
 def test_csr_from_device_arrays(port, name):
     from gpu_spmv_b200 import engine as E
