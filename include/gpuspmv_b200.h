@@ -322,6 +322,26 @@ gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const
                           const double *d_val, const double *d_x, double *d_y,
                           gs_stream stream);
 
+/* K1 SpMV that allocates nothing: y[permi[r]] = row r of the K1 layout times x, FP64, from
+ * the arrays the reference's gk1 kernel takes (cudaSpmv.cu:851), all on the device, in the
+ * str_matK1 layout (chunkNum = ceil(nrows / 32), permi of chunkNum * 32 entries, lenVC
+ * slots of val / col).  No counterpart in the reference: gk1 runs each chunk in one warp
+ * with no scratch; this runs the engine's split-chunk K1 kernel, whose piece partial sums
+ * and arrival counters live in a static device array of 8.25 MiB per device instead of
+ * memory allocated per matrix or per call.  For callers that cannot allocate: ones whose
+ * device memory belongs to another allocator (a framework's caching pool that has
+ * reserved the device), and loops that must not synchronise (cudaFree synchronises the
+ * device).  Layouts above GS_K1_STATIC_MAX_SLOTS slots are refused with
+ * GS_ERR_UNSUPPORTED.  The first call on each device looks the scratch up and zeroes its
+ * counters, synchronising the device: make it before any stream capture or timed loop.
+ * Calls on one device share the scratch, so calls that could overlap (other streams, other
+ * threads) must be serialised by the caller.  Asynchronous on `stream`. */
+#define GS_K1_STATIC_MAX_SLOTS 134217728ull
+gs_status gs_k1_spmv_f64_static(UIN nrows, UIN chunkNum, UIN lenVC, const double *d_val,
+                                const UIN *d_col, const UIN *d_nmc, const UIN *d_chp,
+                                const UIN *d_permi, const double *d_x, double *d_y,
+                                gs_stream stream);
+
 /* Synthetic matrices (host, deterministic for a given seed, any thread count).  Each
  * returns a CSR in malloc'd host arrays the caller frees with gs_free_host. */
 gs_status gs_gen_laplacian2d(UIN grid, UIN **row, UIN **col, double **val, UIN *nrows,
