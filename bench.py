@@ -1,8 +1,9 @@
 #!/usr/bin/env python
 """SpMV benchmark of the B200 engine (one JSON line on stdout, rank 0).
 
-Default workload: FP64 AXT SpMV (the engine's native AXT layout, x gathered at SpMV time)
-on the power-law matrix -- 4,194,304 rows, 67,108,864 nnz, lognormal(2.5, 1.2) row
+Default workload: FP64 SpMV in the K1 format (the engine's fastest FP64 format here; the
+CSR and AXT formats and cuSPARSE are timed in the same run under "formats") on the
+power-law matrix -- 4,194,304 rows, 67,108,864 nnz, lognormal(2.5, 1.2) row
 lengths clipped to [1, 10000] and rescaled, columns uniform without replacement, values
 N(0,1), x uniform[-1,1], seed 1.  A step is one SpMV of the whole matrix (one kernel
 launch).  The value/column streams (805 MB) are larger than the 126 MB L2, so no L2 flush
@@ -69,7 +70,9 @@ VARIANTS = {
     "axt-com-th1-striped": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256,
                                 striped=True),
 }
-DEFAULT_VARIANT = "axt-com-th1"
+DEFAULT_VARIANT = "k1"
+# formats timed beside the headline (µs per product), same matrix and x
+COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc")
 
 
 def make_matrix(workload: str, rank: int):
@@ -185,6 +188,47 @@ def cpu_reference_spmv(row, col, val, x, budget_s=15.0, threads=None):
     dt = (time.perf_counter() - t0) / reps
     nnz = len(col)
     return 2.0 * nnz / dt / 1e9, f"{reps} full SpMVs of the workload ({nnz} nnz)", threads
+
+
+def time_formats(row, col, val, x, steps: int):
+    """µs per product of the other formats and of cuSPARSE CSR on the same matrix and x
+    (per-launch CUDA events, mean over `steps` launches after warm-up)."""
+    import torch
+
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import refapi as R
+
+    n = len(row) - 1
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty(n, dtype=torch.float64, device="cuda")
+    out = {}
+    for vname in COMPARE:
+        kw = dict(VARIANTS[vname])
+        A = E.Matrix(row, col, val, ncols=n, **kw)
+        for _ in range(5):
+            A.spmv(dx, dy)
+        ts = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            A.spmv(dx, dy)
+            b.record()
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        out[vname] = round(1e3 * sum(a.elapsed_time(b) for a, b in ts) / steps, 2)
+        A.close()
+    # cuSPARSE generic CSR SpMV through the drop-in test_gcucsr (per-launch events)
+    h = R.csr_struct(row, col, val)
+    ref = dy.cpu().numpy()
+    old = L.lib().gs_get_num_ite()
+    L.lib().gs_set_num_ite(max(20, steps // 2))
+    try:
+        r = L.lib().test_gcucsr(h.s, R.f64p(x), R.f64p(ref))
+        out["cusparse-csr"] = round(r.et * 1e6, 2) if r.name == b"gcucsr" else None
+    finally:
+        L.lib().gs_set_num_ite(old)
+    return out
 
 
 def run_reference(args):
@@ -357,6 +401,12 @@ def run_ours(args):
                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n, "steps": Ke,
                "path": "gs_spmv_host (C ABI): pinned host x -> device, SpMV, y -> host"}
 
+    formats = None
+    if rank == 0 and world == 1 and not args.no_formats:
+        formats = {"unit": "us per product", "headline": args.variant,
+                   args.variant: round(1e3 * kern, 2)}
+        formats.update(time_formats(row, col, val, x, args.format_steps))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -388,6 +438,7 @@ def run_ours(args):
                      "algorithmic_bytes_per_launch": B, "kernel_ms": kern},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "formats": formats,
         "gpu_launches": K,
         "clocks": clocks,
     }
@@ -407,6 +458,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-formats", action="store_true")
+    ap.add_argument("--format-steps", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
