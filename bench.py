@@ -69,7 +69,43 @@ VARIANTS = {
     "axt-unc-th4-tma": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32, tma=True),
     "axt-com-th1-striped": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256,
                                 striped=True),
+    # mixed precision: FP32 / BF16 values, 32-bit or 16-bit column offsets, FP32 x;
+    # products and sums in FP32, or the sums in FP64 (acc64, FP64 y)
+    "k1-f32": dict(fmt="K1", vtype="f32"),
+    "k1-f32-u16": dict(fmt="K1", vtype="f32", itype="u16"),
+    "k1-f32-u16-acc64": dict(fmt="K1", vtype="f32", itype="u16", acc64=True),
+    "k1-bf16-u16": dict(fmt="K1", vtype="bf16", itype="u16"),
+    "k1-bf16": dict(fmt="K1", vtype="bf16"),
+    "csr-f32": dict(fmt="CSR", vtype="f32"),
+    "csr-f32-u16": dict(fmt="CSR", vtype="f32", itype="u16"),
+    "csr-f32-u16-acc64": dict(fmt="CSR", vtype="f32", itype="u16", acc64=True),
+    "csr-bf16-u16": dict(fmt="CSR", vtype="bf16", itype="u16"),
+    "axt-com-th1-f32-u16": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256,
+                                vtype="f32", itype="u16"),
+    "axt-unc-th1-hw8-f32-u16": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=8, vtype="f32",
+                                    itype="u16"),
+    "axt-unc-th1-hw8-bf16-u16": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=8, vtype="bf16",
+                                     itype="u16"),
 }
+RUN_KEYS = ("tma", "striped", "acc64")
+
+
+def split_variant(vname: str):
+    """(Matrix kwargs, spmv kwargs) of a variant."""
+    kw = dict(VARIANTS[vname])
+    run = {k: kw.pop(k) for k in RUN_KEYS if k in kw}
+    return kw, run
+
+
+def variant_bytes(n: int, nnz: int, kw: dict, run: dict) -> float:
+    from gpu_spmv_b200 import engine as E
+
+    vt = kw.get("vtype", "f64")
+    s_v = {"f64": 8, "f32": 4, "bf16": 2}[vt]
+    s_i = 2 if kw.get("itype") == "u16" else 4
+    s_x = 8 if vt == "f64" else 4
+    s_y = 8 if (vt == "f64" or run.get("acc64")) else 4
+    return E.algorithmic_bytes(n, n, nnz, 1, s_v, s_i, s_x, s_y)
 DEFAULT_VARIANT = "k1"
 # formats timed beside the headline (µs per product), same matrix and x
 COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc")
@@ -188,6 +224,25 @@ def cpu_reference_spmv(row, col, val, x, budget_s=15.0, threads=None):
     dt = (time.perf_counter() - t0) / reps
     nnz = len(col)
     return 2.0 * nnz / dt / 1e9, f"{reps} full SpMVs of the workload ({nnz} nnz)", threads
+
+
+def error_vs_fp64(row, col, val, x, y) -> float:
+    """max_i |y_i - y64_i| / (|A||x|)_i of a reduced-precision product y against the FP64
+    product (the engine's K1 FP64 path, itself within 1e-13 of the reference's CPU loop)."""
+    import torch
+
+    from gpu_spmv_b200 import engine as E
+
+    n = len(row) - 1
+    dx = torch.from_numpy(x).cuda()
+    A = E.Matrix(row, col, val, ncols=n, fmt="K1")
+    y64 = A.spmv(dx)
+    A.close()
+    M = E.Matrix(row, col, np.abs(val), ncols=n, fmt="K1")
+    mag = M.spmv(dx.abs())
+    M.close()
+    r = (y.double() - y64).abs() / mag.clamp_min(1e-300)
+    return float(r.max())
 
 
 def time_formats(row, col, val, x, steps: int):
@@ -315,15 +370,23 @@ def run_ours(args):
     variants = list(VARIANTS) if args.sweep else [args.variant]
     results = {}
     for vname in variants:
-        kw = dict(VARIANTS[vname])
-        tma = kw.pop("tma", False)
-        striped = kw.pop("striped", False)
-        A = E.Matrix(row, col, val, ncols=n, **kw)
+        kw, run = split_variant(vname)
+        try:
+            A = E.Matrix(row, col, val, ncols=n, **kw)
+        except L.GSError as e:
+            if not args.sweep or e.status != L.GS_ERR_UNSUPPORTED:
+                raise
+            print(f"[sweep] {vname:18s} skipped: {e}", file=sys.stderr, flush=True)
+            continue
+        f64 = kw.get("vtype", "f64") == "f64"
         dx = torch.from_numpy(x).cuda()
-        dy = torch.empty(n, dtype=torch.float64, device="cuda")
+        if not f64:
+            dx = dx.float()
+        dy = torch.empty(n, dtype=torch.float64 if (f64 or run.get("acc64")) else torch.float32,
+                         device="cuda")
         stream = torch.cuda.current_stream()
         for _ in range(args.warmup):
-            A.spmv(dx, dy, tma=tma, striped=striped)
+            A.spmv(dx, dy, **run)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
@@ -339,7 +402,7 @@ def run_ours(args):
         ev0.record(stream)
         for k in range(K):
             eb[k].record(stream)
-            A.spmv(dx, dy, tma=tma, striped=striped)
+            A.spmv(dx, dy, **run)
             ea[k].record(stream)
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -353,22 +416,26 @@ def run_ours(args):
             t = torch.tensor([elapsed, kern], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             elapsed, kern = float(t[0]), float(t[1])
-        results[vname] = (A, elapsed, kern, sampler, dx, dy, tma, striped)
+        results[vname] = (A, elapsed, kern, sampler, dx, dy, run)
         if args.sweep and rank == 0:
             gf = 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
-            B = E.algorithmic_bytes(n, n, nnz)
+            B = variant_bytes(n, nnz, kw, run)
+            err = error_vs_fp64(row, col, val, x, dy) if not f64 else 0.0
             print(f"[sweep] {vname:18s} {elapsed / K * 1e3:9.1f} us/step  {gf:8.1f} GFLOP/s  "
                   f"{B / (kern * 1e-3) / 1e9:8.1f} GB/s alg  beta={A.info.beta:.3f} "
-                  f"conv={A.info.conv_ms:.1f} ms", file=sys.stderr, flush=True)
+                  f"conv={A.info.conv_ms:.1f} ms  err={err:.2e}", file=sys.stderr, flush=True)
         if args.sweep:
             A.close()
     if args.sweep:
         return 0
-    A, elapsed, kern, sampler, dx, dy, tma, striped = results[args.variant]
-    spmv_flags = (L.GS_FLAG_TMA if tma else 0) | (L.GS_FLAG_STRIPED if striped else 0)
+    A, elapsed, kern, sampler, dx, dy, run = results[args.variant]
+    kw, _ = split_variant(args.variant)
+    spmv_flags = ((L.GS_FLAG_TMA if run.get("tma") else 0) |
+                  (L.GS_FLAG_STRIPED if run.get("striped") else 0) |
+                  (L.GS_FLAG_ACC_F64 if run.get("acc64") else 0))
     K = args.steps
     value = world * 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
-    B = E.algorithmic_bytes(n, n, nnz)
+    B = variant_bytes(n, nnz, kw, run)
     peak, peak_kind = measured_peak()
     achieved = B / (kern * 1e-3) / 1e9
     tkey = f"{args.workload}/{args.variant}"
@@ -377,28 +444,31 @@ def run_ours(args):
     # ---- end to end through the C ABI with host buffers: H2D x, SpMV, D2H y per step
     e2e = None
     if not args.no_e2e:
-        hx = torch.from_numpy(x).pin_memory()
-        hy = torch.empty(n, dtype=torch.float64).pin_memory()
+        hx = torch.from_numpy(x).to(dx.dtype).pin_memory()
+        hy = torch.empty(n, dtype=dy.dtype).pin_memory()
+        xcode = L.GS_F64 if dx.dtype == torch.float64 else L.GS_F32
+        ycode = L.GS_F64 if dy.dtype == torch.float64 else L.GS_F32
         Ke = min(K, args.e2e_steps)
         lib = L.lib()
         sh = E.stream_handle()
         for _ in range(3):
-            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
-                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, spmv_flags, sh), "e2e")
+            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), xcode,
+                                     hy.data_ptr(), dy.data_ptr(), ycode, spmv_flags, sh), "e2e")
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(Ke):
-            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), L.GS_F64,
-                                     hy.data_ptr(), dy.data_ptr(), L.GS_F64, spmv_flags, sh), "e2e")
+            L.check(lib.gs_spmv_host(A._h, hx.data_ptr(), dx.data_ptr(), xcode,
+                                     hy.data_ptr(), dy.data_ptr(), ycode, spmv_flags, sh), "e2e")
         te = time.perf_counter() - t0
         if dist:
             t = torch.tensor([te], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             te = float(t[0])
         e2e = {"value": world * 2.0 * nnz * Ke / te / 1e9, "unit": "GFLOP/s",
-               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n, "steps": Ke,
+               "h2d_bytes_per_step": hx.element_size() * n,
+               "d2h_bytes_per_step": hy.element_size() * n, "steps": Ke,
                "path": "gs_spmv_host (C ABI): pinned host x -> device, SpMV, y -> host"}
 
     formats = None
@@ -427,9 +497,12 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": elapsed / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": kw.get("vtype", "f64"),
+        "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"],
-                   "format": args.variant, "nrows": n, "nnz": nnz, "beta": info.beta,
+                   "format": args.variant,
+                   "error_vs_fp64": (None if kw.get("vtype", "f64") == "f64" else
+                                     error_vs_fp64(row, col, val, x, dy)), "nrows": n, "nnz": nnz, "beta": info.beta,
                    "l2": "value/column streams > 126 MB L2 each step; no flush",
                    "per_rank": "independent partition of the same size (block-diagonal)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

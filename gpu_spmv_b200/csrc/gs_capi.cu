@@ -122,8 +122,10 @@ gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y
     if (!A || !d_x || !d_y) return gs::fail(GS_ERR_INVALID, "NULL argument");
     cudaStream_t s = gs::cs(stream);
     if (A->p.format == GS_FMT_K1) {
-        if (xtype != GS_F64 || ytype != GS_F64)
-            return gs::fail(GS_ERR_UNSUPPORTED, "K1 takes FP64 x and y");
+        const bool f64 = A->p.vtype == GS_F64;
+        if (xtype != (f64 ? GS_F64 : GS_F32))
+            return gs::fail(GS_ERR_UNSUPPORTED, f64 ? "FP64 matrices take FP64 x"
+                                                    : "FP32/BF16 matrices take FP32 x");
         gs::K1Args a{};
         a.nrows = A->nrows;
         a.chunkNum = A->chunkNum;
@@ -131,16 +133,18 @@ gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y
         a.nmc = A->nmc.as<uint32_t>();
         a.chp = A->chp.as<uint32_t>();
         a.klen = A->k1len.as<uint32_t>();
-        a.val = A->val.as<double>();
-        a.col = A->col.as<uint32_t>();
-        a.x = static_cast<const double *>(d_x);
-        a.y = static_cast<double *>(d_y);
+        a.val = A->val.p;
+        a.col = A->col.p;
+        a.ck = A->k1ck.as<uint32_t>();
+        a.x = d_x;
+        a.y = d_y;
         a.unit_chunk = A->k1unit_chunk.as<uint32_t>();
         a.unit_base = A->k1unit_base.as<uint32_t>();
         a.units = A->k1units;
         a.partial = A->k1partial.as<double>();
         a.count = A->k1count.as<uint32_t>();
-        return gs::launch_k1(a, s);
+        return gs::launch_k1(a, A->p.vtype, A->p.itype, ytype, (flags & GS_FLAG_ACC_F64) != 0,
+                             s);
     }
     const bool f64 = A->p.vtype == GS_F64;
     if (f64 && xtype != GS_F64) return gs::fail(GS_ERR_UNSUPPORTED, "FP64 matrices take FP64 x");

@@ -111,19 +111,37 @@ __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
 }
 
 // one thread per sorted row g of chunk g/32: element e -> chp[c] + 32e + g%32
-template <class VIN>
+template <class VIN, class VOUT>
 __global__ void k_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col,
                           const VIN *val, const uint32_t *permi, const uint32_t *chp,
-                          double *oval, uint32_t *ocol)
+                          VOUT *oval, uint32_t *ocol)
 {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const uint32_t r = permi[g], b = row[r], len = row[r + 1] - b;
     const uint32_t base = chp[g / 32] + (g % 32);
     for (uint32_t e = 0; e < len; e++) {
-        oval[base + 32u * e] = (double)val[b + e];
+        oval[base + 32u * e] = cvt<VIN, VOUT>(val[b + e]);
         ocol[base + 32u * e] = col[b + e];
     }
+}
+
+template <class VIN>
+void launch_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col, const VIN *val,
+                    const uint32_t *permi, const uint32_t *chp, gs_dtype vout, void *oval,
+                    uint32_t *ocol, cudaStream_t s)
+{
+    const unsigned b = (n + 255) / 256;
+    if (vout == GS_F64)
+        k_fill_k1<VIN, double><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+                                                 static_cast<double *>(oval), ocol);
+    else if (vout == GS_F32)
+        k_fill_k1<VIN, float><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+                                                static_cast<float *>(oval), ocol);
+    else
+        k_fill_k1<VIN, __nv_bfloat16><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+                                                        static_cast<__nv_bfloat16 *>(oval),
+                                                        ocol);
 }
 
 __global__ void k_rowlen(uint32_t n, const uint32_t *row, uint32_t *rl)
@@ -219,9 +237,10 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
     if (p.itype == GS_IDX_U16 && p.vtype == GS_F64)
         return fail(GS_ERR_UNSUPPORTED, "16-bit columns need FP32 or BF16 values");
     const bool reduced = p.vtype != GS_F64;
-    if (reduced && !(p.format == GS_FMT_CSR || (p.format == GS_FMT_AXT && p.tileH == 1) ||
-                     p.format == GS_FMT_AXC))
-        return fail(GS_ERR_UNSUPPORTED, "FP32/BF16 storage is available for tileH=1 layouts");
+    if (reduced && !(p.format == GS_FMT_CSR || p.format == GS_FMT_K1 ||
+                     (p.format == GS_FMT_AXT && p.tileH == 1) || p.format == GS_FMT_AXC))
+        return fail(GS_ERR_UNSUPPORTED,
+                    "FP32/BF16 storage is available for CSR, K1, AXC and tileH=1 AXT layouts");
     if ((d_xbake || ax_out) && p.vtype != GS_F64)
         return fail(GS_ERR_UNSUPPORTED, "baked layouts are FP64");
 
@@ -260,8 +279,8 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
     const gs_format fmt = p.format;
 
     if (fmt == GS_FMT_K1) {
-        if (p.vtype != GS_F64 || p.itype != GS_IDX_U32)
-            return fail(GS_ERR_UNSUPPORTED, "K1 is stored as FP64 with 32-bit columns");
+        if (p.vtype == GS_F64 && p.itype != GS_IDX_U32)
+            return fail(GS_ERR_UNSUPPORTED, "FP64 K1 is stored with 32-bit columns");
         const uint32_t chunkNum = (n + 31) / 32;
         A->chunkNum = chunkNum;
         DevBuf rl;
@@ -290,22 +309,41 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
         k_u64_to_u32<<<blocks_for(chunkNum), 256, 0, s>>>(chunkNum, P.as<uint64_t>(),
                                                          A->chp.as<uint32_t>());
         GS_CHECK_LAUNCH();
-        GS_TRY(A->val.alloc_zero((size_t)A->lenVC * 8, s));
-        GS_TRY(A->col.alloc_zero((size_t)A->lenVC * 4, s));
+        const bool u16 = p.itype == GS_IDX_U16;
+        const size_t vsz = dtype_size(p.vtype), isz = u16 ? 2 : 4;
+        GS_TRY(A->val.alloc_zero((size_t)A->lenVC * vsz, s));
+        GS_TRY(A->col.alloc_zero((size_t)A->lenVC * isz, s));
+        DevBuf col32;  // 32-bit columns before the 16-bit steps are taken
+        if (u16) GS_TRY(col32.alloc_zero((size_t)A->lenVC * 4, s));
+        uint32_t *ocol = u16 ? col32.as<uint32_t>() : A->col.as<uint32_t>();
         if (val_type == GS_F64)
-            k_fill_k1<double><<<blocks_for(n), 256, 0, s>>>(
-                n, d_row, d_col, static_cast<const double *>(d_val), A->permi.as<uint32_t>(),
-                A->chp.as<uint32_t>(), A->val.as<double>(), A->col.as<uint32_t>());
+            launch_fill_k1<double>(n, d_row, d_col, static_cast<const double *>(d_val),
+                                   A->permi.as<uint32_t>(), A->chp.as<uint32_t>(), p.vtype,
+                                   A->val.p, ocol, s);
         else
-            k_fill_k1<float><<<blocks_for(n), 256, 0, s>>>(
-                n, d_row, d_col, static_cast<const float *>(d_val), A->permi.as<uint32_t>(),
-                A->chp.as<uint32_t>(), A->val.as<double>(), A->col.as<uint32_t>());
+            launch_fill_k1<float>(n, d_row, d_col, static_cast<const float *>(d_val),
+                                  A->permi.as<uint32_t>(), A->chp.as<uint32_t>(), p.vtype,
+                                  A->val.p, ocol, s);
         GS_CHECK_LAUNCH();
         GS_TRY(build_k1_plan(A->nmc.as<uint32_t>(), chunkNum, A->k1unit_chunk, A->k1unit_base,
                              A->k1partial, A->k1count, &A->k1units, s));
+        if (u16) {
+            K1Args a{};
+            a.nrows = n;
+            a.chunkNum = chunkNum;
+            a.chp = A->chp.as<uint32_t>();
+            a.klen = A->k1len.as<uint32_t>();
+            a.unit_chunk = A->k1unit_chunk.as<uint32_t>();
+            a.unit_base = A->k1unit_base.as<uint32_t>();
+            a.units = A->k1units;
+            GS_TRY(A->k1ck.alloc((size_t)A->k1units * 32 * 4));
+            GS_TRY(build_k1_deltas(a, col32.as<uint32_t>(), A->col.as<uint16_t>(),
+                                   A->k1ck.as<uint32_t>(), s));
+        }
         A->nslots = A->lenVC;
-        A->mfp = (double)chunkNum * 4 + (double)chunkNum * 4 + (double)A->lenVC * 8 +
-                 (double)A->lenVC * 4 + (double)n * 4 + (double)n * 8;
+        A->mfp = (double)chunkNum * 4 + (double)chunkNum * 4 + (double)A->lenVC * vsz +
+                 (double)A->lenVC * isz + (double)n * 4 + (double)n * 8 +
+                 (u16 ? (double)A->k1units * 128 : 0.0);
         A->beta = (double)nnz / (double)A->lenVC;
     } else {
         // ---------------- row-stream layouts

@@ -7,6 +7,7 @@
 
 #include <cstdarg>
 #include <cstddef>
+#include <type_traits>
 
 #include "gpuspmv_b200.h"
 
@@ -143,7 +144,7 @@ struct gs_matrix {
     gs::DevBuf permi, nmc, chp;
     gs::DevBuf rpos, rlen;  // row table for the row-stream kernels
     // K1 execution plan (split of long chunks) and its scratch
-    gs::DevBuf k1len, k1unit_chunk, k1unit_base, k1partial, k1count;
+    gs::DevBuf k1len, k1unit_chunk, k1unit_base, k1partial, k1count, k1ck;
     uint32_t k1units = 0;
     // row-stream kernel configuration
     uint32_t tiled = 0;  // 1: positions map to tile slots (tileH > 1 layouts)
@@ -188,16 +189,21 @@ gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtyp
 struct K1Args {
     uint32_t nrows, chunkNum;
     const uint32_t *permi, *nmc, *chp, *klen;  // klen: per sorted row length or nullptr
-    const double *val;
-    const uint32_t *col;
-    const double *x;
-    double *y;
+    const void *val;  // double / float / __nv_bfloat16
+    const void *col;  // uint32_t columns, or uint16_t steps with checkpoints ck
+    const uint32_t *ck;
+    const void *x;    // double for FP64 values, float otherwise
+    void *y;          // double or float
     const uint32_t *unit_chunk, *unit_base;  // plan
     uint32_t units;
     double *partial;
     uint32_t *count;
 };
-gs_status launch_k1(const K1Args &a, cudaStream_t s);
+gs_status launch_k1(const K1Args &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype, bool acc64,
+                    cudaStream_t s);
+// 16-bit column steps + per-unit checkpoints from 32-bit K1 columns (plan and klen needed).
+gs_status build_k1_deltas(const K1Args &a, const uint32_t *d_col32, uint16_t *d_col16,
+                          uint32_t *d_ck, cudaStream_t s);
 // Build the K1 plan for chunk lengths nmc (device) into the given buffers.
 constexpr uint32_t kK1Split = 256;  // j-steps per K1 work unit
 gs_status build_k1_plan(const uint32_t *d_nmc, uint32_t chunkNum, DevBuf &unit_chunk,

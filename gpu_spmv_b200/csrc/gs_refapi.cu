@@ -561,16 +561,18 @@ str_res test_gk1(const UIN cudaBlockSize, const str_matK1 k, const FPT *vec, con
     a.nmc = nmc.as<UIN>();
     a.chp = chp.as<UIN>();
     a.klen = nullptr;  // struct carries no row lengths: read each chunk's padded width
-    a.val = val.as<double>();
-    a.col = col.as<UIN>();
-    a.x = x.as<double>();
-    a.y = y.as<double>();
+    a.val = val.p;
+    a.col = col.p;
+    a.x = x.p;
+    a.y = y.p;
     a.unit_chunk = uc.as<UIN>();
     a.unit_base = ub.as<UIN>();
     a.units = units;
     a.partial = part.as<double>();
     a.count = cnt.as<UIN>();
-    return timed("gk1", k.nrows, k.nnz, [&]() { return gs::launch_k1(a, 0); }, y, ref);
+    return timed("gk1", k.nrows, k.nnz, [&]() {
+        return gs::launch_k1(a, GS_F64, GS_IDX_U32, GS_F64, false, 0);
+    }, y, ref);
 }
 
 // align: rows start on multiples of `align` positions (UNC tiles / columns, AXC bricks),

@@ -15,14 +15,48 @@
 // (native matrices keep the sorted lengths) and, like gk1, reads the padding otherwise.
 // A chunk whose rows are all empty reads nothing (gk1 reads one slot past it,
 // cudaSpmv.cu:861).
+//
+// Reduced-precision storage (an extension; the reference is FP64 only): values in FP32 or
+// BF16 with FP32 x, products in FP32 and sums in FP32 or FP64; columns either 32-bit or as
+// 16-bit steps from the row's previous column, re-anchored at the first slot of every
+// work unit by a 32-bit checkpoint (ck[unit * 32 + lane]), so each unit decodes its
+// columns with a running sum and no unit depends on another.
 #include "gs_internal.cuh"
 
 namespace gs {
 
 namespace {
 
+template <class T> __device__ __forceinline__ float k1_val_f32(T v);
+template <> __device__ __forceinline__ float k1_val_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ float k1_val_f32<__nv_bfloat16>(__nv_bfloat16 v)
+{
+    return __bfloat162float(v);
+}
+
+// products: FP64 matrices multiply and add in FP64 (non-fused, like the CPU loop); reduced
+// matrices multiply in FP32 and add in AT
+template <class VT, class XT, class AT>
+__device__ __forceinline__ AT k1_fma(AT acc, VT v, XT x)
+{
+    if constexpr (std::is_same<VT, double>::value) {
+        return __dadd_rn(acc, __dmul_rn(v, x));
+    } else {
+        const float p = __fmul_rn(k1_val_f32(v), x);
+        if constexpr (std::is_same<AT, double>::value) return __dadd_rn(acc, (double)p);
+        else return __fadd_rn(acc, p);
+    }
+}
+
+template <class VT, class IT, class AT, class YT>
 __global__ void __launch_bounds__(256) k_k1(const K1Args a)
 {
+    using XT = typename std::conditional<std::is_same<VT, double>::value, double, float>::type;
+    constexpr bool kDelta = std::is_same<IT, uint16_t>::value;
+    const VT *__restrict__ val = static_cast<const VT *>(a.val);
+    const IT *__restrict__ col = static_cast<const IT *>(a.col);
+    const XT *__restrict__ x = static_cast<const XT *>(a.x);
+    YT *__restrict__ y = static_cast<YT *>(a.y);
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
@@ -38,34 +72,47 @@ __global__ void __launch_bounds__(256) k_k1(const K1Args a)
         const uint32_t j0 = piece * kK1Split;
         const uint32_t j1 = min(len, j0 + kK1Split);
         const uint32_t base = __ldg(a.chp + c) + (uint32_t)lane;
-        double acc = 0.0;
+        uint32_t run = 0;  // decoded column of the previous slot (16-bit steps)
+        if constexpr (kDelta) run = j0 < j1 ? __ldg(a.ck + (size_t)u * 32 + lane) : 0u;
+        AT acc = AT(0);
         uint32_t j = j0;
         // 8 slots in flight per lane: loads first, then gathers, then the ordered sum
         for (; j + 8 <= j1; j += 8) {
-            double v[8], xv[8];
-            uint32_t c[8];
+            VT v[8];
+            XT xv[8];
+            uint32_t cc[8];
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const uint32_t pos = base + 32u * (j + u);
-                v[u] = __ldcs(a.val + pos);
-                c[u] = __ldcs(a.col + pos);
+            for (int k = 0; k < 8; k++) {
+                const uint32_t pos = base + 32u * (j + k);
+                v[k] = __ldcs(val + pos);
+                cc[k] = (uint32_t)__ldcs(col + pos);
+            }
+            if constexpr (kDelta) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    run += cc[k];
+                    cc[k] = run;
+                }
             }
 #pragma unroll
-            for (int u = 0; u < 8; u++) xv[u] = __ldg(a.x + c[u]);
+            for (int k = 0; k < 8; k++) xv[k] = __ldg(x + cc[k]);
 #pragma unroll
-            for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, __dmul_rn(v[u], xv[u]));
+            for (int k = 0; k < 8; k++) acc = k1_fma<VT, XT, AT>(acc, v[k], xv[k]);
         }
         for (; j < j1; j++) {
             const uint32_t pos = base + 32u * j;
-            const double v = __ldcs(a.val + pos);
-            const double xv = __ldg(a.x + __ldcs(a.col + pos));
-            acc = __dadd_rn(acc, __dmul_rn(v, xv));
+            uint32_t cj = (uint32_t)__ldcs(col + pos);
+            if constexpr (kDelta) {
+                run += cj;
+                cj = run;
+            }
+            acc = k1_fma<VT, XT, AT>(acc, __ldcs(val + pos), __ldg(x + cj));
         }
         if (np == 1) {
-            if (valid) a.y[__ldg(a.permi + g)] = acc;
+            if (valid) y[__ldg(a.permi + g)] = (YT)acc;
             continue;
         }
-        a.partial[(size_t)u * 32 + lane] = acc;
+        a.partial[(size_t)u * 32 + lane] = (double)acc;
         __threadfence();
         __syncwarp();
         uint32_t ticket = 0;
@@ -73,12 +120,47 @@ __global__ void __launch_bounds__(256) k_k1(const K1Args a)
         ticket = __shfl_sync(0xffffffffu, ticket, 0);
         if (ticket == np - 1) {
             __threadfence();
-            double s = 0.0;
-            for (uint32_t k = 0; k < np; k++)
-                s = __dadd_rn(s, __ldcg(a.partial + (size_t)(ub + k) * 32 + lane));
-            if (valid) a.y[__ldg(a.permi + g)] = s;
+            AT s = AT(0);
+            for (uint32_t k = 0; k < np; k++) {
+                const AT pk = (AT)__ldcg(a.partial + (size_t)(ub + k) * 32 + lane);
+                if constexpr (std::is_same<AT, double>::value) s = __dadd_rn(s, pk);
+                else s = __fadd_rn(s, pk);
+            }
+            if (valid) y[__ldg(a.permi + g)] = (YT)s;
             if (lane == 0) a.count[c] = 0;  // ready for the next launch
         }
+    }
+}
+
+// 16-bit column steps: for unit u and lane l, ck = column of the unit's first slot,
+// col16 = column - previous column inside the unit (0 at the first slot); flag bit 0 when
+// a step is negative or above 65535.
+__global__ void __launch_bounds__(256) k_k1_deltas(const K1Args a, const uint32_t *col32,
+                                                   uint16_t *col16, uint32_t *ck,
+                                                   uint32_t *flag)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
+         u += warps) {
+        const uint32_t c = a.unit_chunk[u];
+        const uint32_t piece = u - a.unit_base[c];
+        const uint32_t g = 32u * c + (uint32_t)lane;
+        const uint32_t len = g < a.nrows ? a.klen[g] : 0u;
+        const uint32_t j0 = piece * kK1Split;
+        const uint32_t j1 = min(len, j0 + kK1Split);
+        const uint32_t base = a.chp[c] + (uint32_t)lane;
+        uint32_t prev = j0 < j1 ? col32[base + 32u * j0] : 0u;
+        ck[(size_t)u * 32 + lane] = prev;
+        bool bad = false;
+        for (uint32_t j = j0; j < j1; j++) {
+            const uint32_t cj = col32[base + 32u * j];
+            const uint32_t d = cj - prev;  // wraps when the row's columns decrease
+            bad |= d > 0xffffu;
+            col16[base + 32u * j] = (uint16_t)d;
+            prev = cj;
+        }
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, 1u);
     }
 }
 
@@ -120,13 +202,66 @@ gs_status build_k1_plan(const uint32_t *d_nmc, uint32_t chunkNum, DevBuf &unit_c
     return GS_OK;
 }
 
-gs_status launch_k1(const K1Args &a, cudaStream_t s)
+namespace {
+uint32_t k1_blocks(uint32_t units) { return min((units + 7) / 8, 148u * 64u); }
+
+template <class VT, class IT, class AT, class YT>
+gs_status launch_k1_t(const K1Args &a, cudaStream_t s)
+{
+    k_k1<VT, IT, AT, YT><<<k1_blocks(a.units), 256, 0, s>>>(a);
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
+template <class VT, class IT>
+gs_status launch_k1_acc(const K1Args &a, bool acc64, gs_dtype ytype, cudaStream_t s)
+{
+    if (acc64) {
+        if (ytype == GS_F64) return launch_k1_t<VT, IT, double, double>(a, s);
+        return launch_k1_t<VT, IT, double, float>(a, s);
+    }
+    if (ytype == GS_F64) return launch_k1_t<VT, IT, float, double>(a, s);
+    return launch_k1_t<VT, IT, float, float>(a, s);
+}
+}  // namespace
+
+gs_status launch_k1(const K1Args &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype, bool acc64,
+                    cudaStream_t s)
 {
     if (a.units == 0) return GS_OK;
-    uint32_t blocks = (a.units + 7) / 8;
-    blocks = min(blocks, 148u * 64u);
-    k_k1<<<blocks, 256, 0, s>>>(a);
+    if (itype == GS_IDX_U16 && !a.ck) return fail(GS_ERR_INVALID, "16-bit K1 without checkpoints");
+    if (vtype == GS_F64) {
+        if (itype != GS_IDX_U32 || ytype != GS_F64)
+            return fail(GS_ERR_UNSUPPORTED, "FP64 K1 takes 32-bit columns and FP64 y");
+        return launch_k1_t<double, uint32_t, double, double>(a, s);
+    }
+    if (vtype == GS_F32) {
+        if (itype == GS_IDX_U16) return launch_k1_acc<float, uint16_t>(a, acc64, ytype, s);
+        return launch_k1_acc<float, uint32_t>(a, acc64, ytype, s);
+    }
+    if (vtype == GS_BF16) {
+        if (itype == GS_IDX_U16) return launch_k1_acc<__nv_bfloat16, uint16_t>(a, acc64, ytype, s);
+        return launch_k1_acc<__nv_bfloat16, uint32_t>(a, acc64, ytype, s);
+    }
+    return fail(GS_ERR_UNSUPPORTED, "value type %d", (int)vtype);
+}
+
+gs_status build_k1_deltas(const K1Args &a, const uint32_t *d_col32, uint16_t *d_col16,
+                          uint32_t *d_ck, cudaStream_t s)
+{
+    if (a.units == 0) return GS_OK;
+    DevBuf flag;
+    GS_TRY(flag.alloc_zero(4, s));
+    k_k1_deltas<<<k1_blocks(a.units), 256, 0, s>>>(a, d_col32, d_col16, d_ck,
+                                                     flag.as<uint32_t>());
     GS_CHECK_LAUNCH();
+    uint32_t hf = 0;
+    GS_CUDA(cudaMemcpyAsync(&hf, flag.p, 4, cudaMemcpyDeviceToHost, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    if (hf)
+        return fail(GS_ERR_UNSUPPORTED,
+                    "a row's consecutive columns are more than 65535 apart (or decrease): "
+                    "16-bit K1 column steps do not fit this matrix");
     return GS_OK;
 }
 

@@ -1160,9 +1160,10 @@ __global__ void k_split_rows(uint32_t n, const uint32_t *rpos, const uint64_t *p
 
 // per window: min column over real positions -> base; flag if the spread exceeds 16 bits;
 // then col16 = col32 - base (padding slots keep 0)
-__global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, const uint32_t *col32,
-                           const uint32_t *rbits, uint32_t *colbase, uint16_t *col16,
-                           uint32_t *flag)
+// nreal: slots at or past it hold no element (the tail of a compact layout's last tile)
+__global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, uint32_t nreal,
+                           const uint32_t *col32, const uint32_t *rbits, uint32_t *colbase,
+                           uint16_t *col16, uint32_t *flag)
 {
     const int lane = threadIdx.x & 31;
     for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nwin;
@@ -1170,7 +1171,7 @@ __global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, const ui
         const uint32_t b = w * WS, e = min(b + WS, nslots);
         uint32_t mn = 0xffffffffu, mx = 0;
         for (uint32_t s = b + lane; s < e; s += 32) {
-            const bool real = !rbits || ((rbits[s >> 5] >> (s & 31)) & 1u);
+            const bool real = s < nreal && (!rbits || ((rbits[s >> 5] >> (s & 31)) & 1u));
             if (real) { mn = min(mn, col32[s]); mx = max(mx, col32[s]); }
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -1183,7 +1184,7 @@ __global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, const ui
             if (mn != 0xffffffffu && mx - mn > 65535u) atomicOr(flag, 1u);
         }
         for (uint32_t s = b + lane; s < e; s += 32) {
-            const bool real = !rbits || ((rbits[s >> 5] >> (s & 31)) & 1u);
+            const bool real = s < nreal && (!rbits || ((rbits[s >> 5] >> (s & 31)) & 1u));
             col16[s] = real ? (uint16_t)(col32[s] - base) : (uint16_t)0;
         }
     }
@@ -1255,7 +1256,8 @@ gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &
     GS_TRY(flag.alloc_zero(4, s));
     const uint32_t blocks = min((P.nwin + 7) / 8, 148u * 64u);
     if (blocks)
-        k_u16_cols<<<blocks, 256, 0, s>>>(P.nwin, 32u * P.V, nslots, d_col32,
+        k_u16_cols<<<blocks, 256, 0, s>>>(P.nwin, 32u * P.V, nslots,
+                                          P.padded ? nslots : min(P.npos, nslots), d_col32,
                                           P.padded ? P.rbits.as<uint32_t>() : nullptr,
                                           P.colbase.as<uint32_t>(), d_col16, flag.as<uint32_t>());
     GS_CHECK_LAUNCH();

@@ -1,0 +1,119 @@
+"""Reduced-precision storage on the GPU: FP32 or BF16 values, 32-bit or 16-bit column
+offsets, FP32 x, products in FP32 and row sums in FP32 or FP64.  Each product is checked
+row by row against the exact (long double) CSR product of the FP64 matrix and FP64 x:
+
+    |y_i - y_i^exact| <= tol_i * (|A||x|)_i,
+    tol_i = u_v + 2^-24 (2 + len_i)        FP32 sums (len_i FP32 additions)
+    tol_i = u_v + 2^-24 * 3                FP64 sums of FP32 products
+    u_v   = 2^-24 (FP32 values) or 2^-8 (BF16 values, round to nearest even)
+
+(value rounding, x rounding, product rounding and the sums; the final rounding of an FP32
+y adds one more 2^-24 and is inside the 2 + len_i and 3 terms)."""
+import numpy as np
+import pytest
+import torch
+
+from mats import case
+
+pytestmark = pytest.mark.gpu
+
+LAYOUTS = [("CSR", {}), ("K1", {}), ("AXC", {"hbs": 32}),
+           ("AXT", dict(mode="UNC", tileH=1, tileHW=8)),
+           ("AXT", dict(mode="UNC", tileH=1, tileHW=4)),
+           ("AXT", dict(mode="COM", tileH=1, tileHW=32, bs=256))]
+U32 = 2.0 ** -24
+
+
+def _ids(p):
+    f, kw = p
+    return f + "".join(f"_{k}{v}" for k, v in kw.items())
+
+
+def _bf16_round(a: np.ndarray) -> np.ndarray:
+    """FP64 -> BF16 (8 significant bits, round to nearest even) -> FP64, for normal values:
+    scale by the power-of-two spacing of the value's binade, round, scale back (all exact)."""
+    a = np.asarray(a, np.float64)
+    _, e = np.frexp(a)  # a = m 2^e, 0.5 <= |m| < 1
+    ulp = np.ldexp(1.0, e - 8)
+    return np.where(a == 0, a, np.rint(a / ulp) * ulp)
+
+
+@pytest.mark.parametrize("name", ["mixed", "row0_empty", "dense_row", "powerlaw_small",
+                                  "laplacian"])
+@pytest.mark.parametrize("layout", LAYOUTS, ids=[_ids(p) for p in LAYOUTS])
+@pytest.mark.parametrize("vtype", ["f32", "bf16"])
+@pytest.mark.parametrize("itype", ["u32", "u16"])
+@pytest.mark.parametrize("acc", ["f32", "f64"])
+def test_reduced_precision_bound(port, name, layout, vtype, itype, acc):
+    from gpu_spmv_b200 import engine as E
+
+    fmt, kw = layout
+    rng = np.random.default_rng(sum(map(ord, name)) + 5)
+    row, col, val = case(name, rng)
+    n = len(row) - 1
+    ncols = max(n, int(col.max()) + 1)
+    A = E.Matrix(row, col, val, ncols=ncols, fmt=fmt, vtype=vtype, itype=itype, **kw)
+    xh = rng.uniform(-1, 1, ncols)
+    x = torch.from_numpy(xh).float().cuda()
+    y = A.spmv(x, acc64=(acc == "f64")).cpu().numpy().astype(np.float64)
+    assert y.dtype == np.float64 and len(y) == n
+    exact, mag = port.csr_truth(row, col, val, xh)
+    lens = np.diff(row).astype(np.float64)
+    u_v = U32 if vtype == "f32" else 2.0 ** -8
+    tol = u_v + U32 * ((2 + lens) if acc == "f32" else 3)
+    err = np.abs(y - exact)
+    assert np.all(err <= tol * mag), float(np.max(err / np.maximum(tol * mag, 1e-300)))
+    # the stored values are the rounded FP64 values, in the same slots as FP64 storage
+    ref = E.Matrix(row, col, val, ncols=ncols, fmt=fmt, **kw).layout()["val"]
+    got = A.layout()["val"]
+    if vtype == "f32":
+        assert np.array_equal(got, ref.astype(np.float32))
+    else:
+        want = _bf16_round(ref)
+        got64 = (got.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+        assert np.array_equal(got64, want)
+    A.close()
+
+
+@pytest.mark.parametrize("acc", ["f32", "f64"])
+def test_fp32_sums_of_fp64_values_close(port, acc):
+    """FP32 storage of the 27-point stencil values (-1 +- 0.1 off the diagonal, 26 on it)
+    keeps the relative error below 1e-6 of (|A||x|)_i."""
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    row, col, val = matgen.stencil27(24, seed=2)
+    n = len(row) - 1
+    xh = matgen.vector(n, "normal", seed=2)
+    A = E.Matrix(row, col, val, fmt="CSR", vtype="f32", itype="u16")
+    y = A.spmv(torch.from_numpy(xh).float().cuda(), acc64=(acc == "f64")).cpu().numpy()
+    exact, mag = port.csr_truth(row, col, val, xh)
+    assert np.max(np.abs(y.astype(np.float64) - exact) / mag) < 1e-6
+
+
+def test_u16_offsets_refused_when_a_window_spans_too_many_columns():
+    from gpu_spmv_b200 import GSError
+    from gpu_spmv_b200 import engine as E
+
+    n = 4096
+    row = np.arange(n + 1, dtype=np.uint32)
+    col = ((np.arange(n, dtype=np.uint64) * 7919 * 64) % (1 << 22)).astype(np.uint32)
+    val = np.ones(n)
+    with pytest.raises(GSError, match="16-bit column offsets"):
+        E.Matrix(row, col, val, ncols=1 << 22, fmt="CSR", vtype="f32", itype="u16")
+
+
+def test_k1_u16_steps_refused_when_columns_are_far_apart():
+    from gpu_spmv_b200 import GSError
+    from gpu_spmv_b200 import engine as E
+
+    n = 64
+    row = np.arange(0, 2 * n + 1, 2, dtype=np.uint32)
+    col = np.stack([np.arange(n), 70000 + np.arange(n)], 1).reshape(-1).astype(np.uint32)
+    val = np.ones(2 * n)
+    with pytest.raises(GSError, match="16-bit K1 column steps"):
+        E.Matrix(row, col, val, ncols=70000 + n, fmt="K1", vtype="f32", itype="u16")
+    # 32-bit columns take it
+    A = E.Matrix(row, col, val, ncols=70000 + n, fmt="K1", vtype="f32")
+    y = A.spmv(torch.ones(70000 + n, dtype=torch.float32, device="cuda"))
+    assert torch.equal(y, torch.full((n,), 2.0, device="cuda"))
