@@ -245,6 +245,107 @@ def error_vs_fp64(row, col, val, x, y) -> float:
     return float(r.max())
 
 
+def _time_us(fn, steps: int, warm: int = 5) -> float:
+    """Mean µs of fn() over `steps` calls, CUDA events around each call (current stream)."""
+    import torch
+
+    for _ in range(warm):
+        fn()
+    evs = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    return 1e3 * sum(a.elapsed_time(b) for a, b in evs) / steps
+
+
+def time_mixed(steps: int):
+    """27-point stencil 160^3: FP64 K1 against reduced-precision K1 (µs per product, GFLOP/s,
+    max_i |y - y64|_i / (|A||x|)_i)."""
+    import torch
+
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    row, col, val = matgen.stencil27(160, seed=2)
+    n, nnz = len(row) - 1, len(col)
+    x = matgen.vector(n, "normal", seed=2)
+    out = {"workload": "27-point stencil 160^3 (4096000 rows, %d nnz), x N(0,1), seed 2" % nnz}
+    dx64 = torch.from_numpy(x).cuda()
+    for name, kw, acc in (("k1-f64", {}, False), ("k1-f32", dict(vtype="f32"), False),
+                          ("k1-f32-acc64", dict(vtype="f32"), True),
+                          ("k1-bf16", dict(vtype="bf16"), False)):
+        A = E.Matrix(row, col, val, ncols=n, fmt="K1", **kw)
+        dx = dx64 if not kw else dx64.float()
+        y = torch.empty(n, dtype=torch.float64 if (not kw or acc) else torch.float32,
+                        device="cuda")
+        us = _time_us(lambda: A.spmv(dx, y, acc64=acc), steps)
+        err = 0.0 if not kw else error_vs_fp64(row, col, val, x, y)
+        out[name] = {"us": round(us, 2), "gflops": round(2.0 * nnz / us / 1e3, 1),
+                     "error_vs_fp64": err}
+        A.close()
+    out["speedup_f32_vs_f64"] = round(out["k1-f64"]["us"] / out["k1-f32"]["us"], 3)
+    return out
+
+
+def time_adjoint(steps: int):
+    """Differentiable product Y = A(v) X, FP32, 8 right-hand sides, on a power-law matrix of
+    1,048,576 rows and 16,777,216 nnz (lognormal(2.5, 1.2) lengths, seed 4): forward,
+    adjoint (Xbar and vbar) in both modes, and the (forward + adjoint) / forward ratio."""
+    import torch
+
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    row, col, val = matgen.powerlaw(nrows=1048576, nnz=16777216, seed=4)
+    n, nnz, k = len(row) - 1, len(col), 8
+    g = torch.Generator(device="cuda").manual_seed(4)
+    A = E.Matrix(row, col, val, ncols=n, fmt="K1", vtype="f32", adjoint=True)
+    X = torch.randn(n, k, device="cuda", generator=g)
+    B = torch.randn(n, k, device="cuda", generator=g)
+    Y = torch.empty(n, k, device="cuda")
+    Xbar = torch.empty(n, k, device="cuda")
+    vbar = torch.empty(nnz, device="cuda")
+    Yb = A.spmm(X) - B
+    from gpu_spmv_b200 import _lib as L
+
+    lib, sh = L.lib(), E.stream_handle()
+
+    def fwd():
+        L.check(lib.gs_spmm(A._h, X.data_ptr(), Y.data_ptr(), L.GS_F32, k, sh), "spmm")
+
+    vslots = torch.empty(A.value_slots(), device="cuda")
+
+    def adj(mode, order):
+        vb = vslots if order == L.GS_VALUES_SLOTS else vbar
+        L.check(lib.gs_spmm_adjoint(A._h, Yb.data_ptr(), X.data_ptr(), Xbar.data_ptr(),
+                                    vb.data_ptr(), L.GS_F32, k, mode, order, sh), "adjoint")
+
+    vals = torch.from_numpy(val.astype(np.float32)).cuda()
+    vals_slots = A.convert_values(vals, to="slots")
+    f = _time_us(fwd, steps)
+    ads = _time_us(lambda: adj(L.GS_ADJ_DETERMINISTIC, L.GS_VALUES_SLOTS), steps)
+    adc = _time_us(lambda: adj(L.GS_ADJ_DETERMINISTIC, L.GS_VALUES_CSR), steps)
+    aa = _time_us(lambda: adj(L.GS_ADJ_ATOMIC, L.GS_VALUES_CSR), steps)
+    svs = _time_us(lambda: A.set_values(vals_slots, "slots"), steps)
+    svc = _time_us(lambda: A.set_values(vals, "csr"), steps)
+    A.close()
+    return {"workload": "power-law 1048576 rows x %d nnz, FP32 values, 8 RHS, seed 4" % nnz,
+            "forward_us": round(f, 2), "forward_gflops": round(2.0 * nnz * k / f / 1e3, 1),
+            "adjoint_deterministic_slots_us": round(ads, 2),
+            "adjoint_deterministic_csr_us": round(adc, 2),
+            "adjoint_atomic_csr_us": round(aa, 2),
+            "set_values_slots_us": round(svs, 2), "set_values_csr_us": round(svc, 2),
+            "fwd_plus_adj_over_fwd": round((f + ads) / f, 3),
+            "fwd_plus_adj_over_fwd_csr_order": round((f + adc) / f, 3),
+            "fwd_plus_adj_over_fwd_atomic": round((f + aa) / f, 3),
+            "note": "adjoint = Xbar = A^T Ybar and vbar (value gradient) in one launch; "
+                    "slots = values kept in the adjoint layout's order"}
+
+
 def time_formats(row, col, val, x, steps: int):
     """µs per product of the other formats and of cuSPARSE CSR on the same matrix and x
     (per-launch CUDA events, mean over `steps` launches after warm-up)."""
@@ -477,6 +578,12 @@ def run_ours(args):
                    args.variant: round(1e3 * kern, 2)}
         formats.update(time_formats(row, col, val, x, args.format_steps))
 
+    mixed = adjoint = None
+    if rank == 0 and world == 1 and not args.no_mixed:
+        mixed = time_mixed(args.format_steps)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = time_adjoint(args.format_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -512,6 +619,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "formats": formats,
+        "mixed": mixed,
+        "adjoint": adjoint,
         "gpu_launches": K,
         "clocks": clocks,
     }
@@ -532,6 +641,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-formats", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--format-steps", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()

@@ -6,12 +6,13 @@ Layers:
     device API (gs_*);
   * ``engine``: device-resident matrices (CSR / K1 / AXC / AXT) and SpMV from Python;
   * ``matgen``: seeded synthetic workloads;
-  * ``refapi``: ctypes helpers for the drop-in layer.
+  * ``refapi``: ctypes helpers for the drop-in layer;
+  * ``autograd``: Y = A(v) X as a torch.autograd.Function over the hand-written adjoint.
 """
 from . import _lib
 from ._lib import GSError, lib
 
-__all__ = ["GSError", "lib", "engine", "matgen", "refapi", "version"]
+__all__ = ["GSError", "lib", "engine", "matgen", "refapi", "autograd", "version"]
 
 
 def version() -> str:
@@ -19,7 +20,7 @@ def version() -> str:
 
 
 def __getattr__(name):
-    if name in ("engine", "matgen", "refapi"):
+    if name in ("engine", "matgen", "refapi", "autograd"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)

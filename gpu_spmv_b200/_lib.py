@@ -27,6 +27,8 @@ GS_FMT_CSR, GS_FMT_K1, GS_FMT_AXC, GS_FMT_AXT = 0, 1, 2, 3
 GS_AXT_UNC, GS_AXT_COM = 0, 1
 GS_FLAG_NONE, GS_FLAG_ACC_F64, GS_FLAG_TMA, GS_FLAG_STRIPED = 0, 1, 2, 4
 GS_K1_STATIC_MAX_SLOTS = 134217728
+GS_ADJ_DETERMINISTIC, GS_ADJ_ATOMIC = 0, 1
+GS_VALUES_CSR, GS_VALUES_SLOTS = 0, 1
 
 
 # ------------------------------------------------------------------ drop-in structs
@@ -129,6 +131,12 @@ SIGNATURES = {
     "gs_spmv_host": (_st, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_int, UIN, _vp]),
     "gs_csr_spmv_f64": (_st, [UIN, UIN, UIN, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gs_k1_spmv_f64_static": (_st, [UIN, UIN, UIN, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gs_spmm": (_st, [_vp, _vp, _vp, C.c_int, UIN, _vp]),
+    "gs_matrix_prepare_adjoint": (_st, [_vp, _vp, _vp, _vp]),
+    "gs_matrix_set_values": (_st, [_vp, _vp, C.c_int, C.c_int, _vp]),
+    "gs_matrix_value_slots": (_st, [_vp, C.POINTER(UIN)]),
+    "gs_matrix_convert_values": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, _vp]),
+    "gs_spmm_adjoint": (_st, [_vp, _vp, _vp, _vp, _vp, C.c_int, UIN, C.c_int, C.c_int, _vp]),
     "gs_copy_to_host": (_st, [_vp, _vp, C.c_size_t]),
     "gs_matrix_device_status": (_st, [_vp, C.POINTER(UIN), C.c_int]),
     "gs_gen_laplacian2d": (_st, [UIN, C.POINTER(UINp), C.POINTER(UINp), C.POINTER(FPTp),

@@ -145,6 +145,15 @@ struct gs_matrix {
     gs::DevBuf rpos, rlen;  // row table for the row-stream kernels
     // K1 execution plan (split of long chunks) and its scratch
     gs::DevBuf k1len, k1unit_chunk, k1unit_base, k1partial, k1count, k1ck;
+    // multi-RHS products (gs_spmm) and the adjoint (gs_matrix_prepare_adjoint)
+    gs::DevBuf mmpartial;  // split pieces x 32 lanes x up to 32 RHS (FP64 sized)
+    uint32_t k1split_units = 0;
+    bool mm_ready = false, adj_ready = false;
+    gs::DevBuf fsrc;    // forward slot -> CSR index
+    gs::DevBuf ftslot;  // forward slot -> adjoint-layout slot
+    gs::DevBuf tpermi, tnmc, tchp, tlen, trow, tsrc, tval;  // K1 layout of A^T
+    gs::DevBuf tunit_chunk, tunit_base, tpartial1, tcount, tpartial;
+    uint32_t tchunkNum = 0, tlenVC = 0, tunits = 0, tsplit_units = 0;
     uint32_t k1units = 0;
     // row-stream kernel configuration
     uint32_t tiled = 0;  // 1: positions map to tile slots (tileH > 1 layouts)

@@ -50,7 +50,7 @@ class Matrix:
 
     def __init__(self, row, col, val, ncols=None, fmt="CSR", tileHW=32, tileH=1, bs=256,
                  mode="COM", hbs=32, vtype="f64", itype="u32", keep_layout=False,
-                 device="cuda", stream=None):
+                 device="cuda", stream=None, adjoint=False):
         self._h = None
         dev = torch.device(device)
         row_t = to_device_u32(row, dev)
@@ -76,6 +76,12 @@ class Matrix:
         self._h = h
         self.device = dev
         self.info = self._info()
+        self._values_key = None
+        if adjoint:
+            with torch.cuda.device(dev):
+                L.check(L.lib().gs_matrix_prepare_adjoint(h, row_t.data_ptr(), col_t.data_ptr(),
+                                                          stream_handle(stream)),
+                        "gs_matrix_prepare_adjoint")
 
     def _info(self) -> L.MatrixInfo:
         i = L.MatrixInfo()
@@ -103,6 +109,128 @@ class Matrix:
         L.check(L.lib().gs_spmv(self._h, x.data_ptr(), xcode, y.data_ptr(), ycode, flags,
                                 stream_handle(stream)), "gs_spmv")
         return y
+
+    # ---------------------------------------------------------------- multi-RHS / adjoint
+    MM_K = (1, 2, 4, 8, 16, 32)
+
+    def _value_dtype(self):
+        if self.vtype not in (L.GS_F64, L.GS_F32):
+            raise TypeError("multi-RHS products take FP64 or FP32 matrices")
+        return TORCH_DTYPES[self.vtype]
+
+    @classmethod
+    def _blocks(cls, k: int):
+        """Column blocks of at most 32 right-hand sides, each padded to a supported width."""
+        out, c0 = [], 0
+        while c0 < k:
+            w = min(32, k - c0)
+            kp = next(q for q in cls.MM_K if q >= w)
+            out.append((c0, w, kp))
+            c0 += w
+        return out
+
+    def spmm(self, X: torch.Tensor, stream=None) -> torch.Tensor:
+        """Y = A X for X of shape [ncols, k] (any k; run in blocks of up to 32 columns)."""
+        dt = self._value_dtype()
+        if X.dim() == 1:
+            return self.spmm(X[:, None], stream)[:, 0]
+        if X.dtype != dt or not X.is_cuda or X.shape[0] != self.ncols:
+            raise TypeError(f"X must be a CUDA {dt} tensor with {self.ncols} rows")
+        k = X.shape[1]
+        Y = torch.empty(self.nrows, k, dtype=dt, device=X.device)
+        for c0, w, kp in self._blocks(k):
+            Xb = X[:, c0:c0 + w]
+            if kp != w or not Xb.is_contiguous() or Xb.data_ptr() % 32:
+                Xp = torch.zeros(self.ncols, kp, dtype=dt, device=X.device)
+                Xp[:, :w] = Xb
+                Xb = Xp
+            Yb = Y[:, c0:c0 + w] if (kp == w and w == k) else \
+                torch.empty(self.nrows, kp, dtype=dt, device=X.device)
+            L.check(L.lib().gs_spmm(self._h, Xb.data_ptr(), Yb.data_ptr(), self.vtype, kp,
+                                    stream_handle(stream)), "gs_spmm")
+            if Yb.data_ptr() != Y.data_ptr():
+                Y[:, c0:c0 + w] = Yb[:, :w]
+        return Y
+
+    ORDERS = {"csr": L.GS_VALUES_CSR, "slots": L.GS_VALUES_SLOTS}
+
+    def value_slots(self) -> int:
+        """Length of a value array in "slots" order (the adjoint layout's slots)."""
+        n = L.UIN()
+        L.check(L.lib().gs_matrix_value_slots(self._h, C.byref(n)), "gs_matrix_value_slots")
+        return n.value
+
+    def _order_len(self, order: str) -> int:
+        return self.nnz if order == "csr" else self.value_slots()
+
+    def set_values(self, values: torch.Tensor, order: str = "csr", stream=None):
+        """Replace the stored values by `values`: nnz entries in the CSR order of creation
+        ("csr") or value_slots() entries in the adjoint layout's order ("slots"); needs a
+        matrix created with adjoint=True."""
+        dt = self._value_dtype()
+        if values.dtype != dt or not values.is_cuda or values.numel() != self._order_len(order):
+            raise TypeError(f"values must be {self._order_len(order)} CUDA {dt} entries")
+        v = values.contiguous()
+        L.check(L.lib().gs_matrix_set_values(self._h, v.data_ptr(), self.vtype,
+                                             self.ORDERS[order], stream_handle(stream)),
+                "gs_matrix_set_values")
+        self._values_key = (v.data_ptr(), getattr(values, "_version", None), order)
+
+    def convert_values(self, values: torch.Tensor, to: str, stream=None) -> torch.Tensor:
+        """The same values in the other order ("csr" <-> "slots")."""
+        src = "slots" if to == "csr" else "csr"
+        dt = self._value_dtype()
+        v = values.contiguous()
+        if v.dtype != dt or v.numel() != self._order_len(src):
+            raise TypeError(f"expected {self._order_len(src)} {dt} values in {src} order")
+        out = torch.zeros(self._order_len(to), dtype=dt, device=v.device)
+        L.check(L.lib().gs_matrix_convert_values(self._h, v.data_ptr(), self.ORDERS[src],
+                                                 out.data_ptr(), self.vtype,
+                                                 stream_handle(stream)),
+                "gs_matrix_convert_values")
+        return out
+
+    def adjoint(self, Ybar: torch.Tensor, X: torch.Tensor | None = None, mode="deterministic",
+                want_vbar: bool = True, order: str = "csr", stream=None):
+        """(Xbar, vbar): Xbar = A^T Ybar, vbar[e] = Ybar[row_e] . X[col_e] in `order` ("csr"
+        or "slots"; None unless want_vbar).  mode "deterministic" (transposed layout) or
+        "atomic"."""
+        dt = self._value_dtype()
+        if Ybar.dim() == 1:
+            Xb, vb = self.adjoint(Ybar[:, None], None if X is None else X[:, None], mode,
+                                  want_vbar, order, stream)
+            return Xb[:, 0], vb
+        k = Ybar.shape[1]
+        m = L.GS_ADJ_ATOMIC if mode == "atomic" else L.GS_ADJ_DETERMINISTIC
+        if m == L.GS_ADJ_ATOMIC:
+            want_vbar = True
+        if want_vbar and X is None:
+            raise TypeError("vbar needs X")
+        Xbar = torch.empty(self.ncols, k, dtype=dt, device=Ybar.device)
+        nv = self._order_len(order)
+        vbar = torch.zeros(nv, dtype=dt, device=Ybar.device) if want_vbar else None
+        part = torch.zeros(nv, dtype=dt, device=Ybar.device) if want_vbar else None
+        blocks = self._blocks(k)
+        for i, (c0, w, kp) in enumerate(blocks):
+            def padded(T, rows):
+                Tb = T[:, c0:c0 + w]
+                if kp == w and Tb.is_contiguous() and Tb.data_ptr() % 32 == 0:
+                    return Tb
+                P = torch.zeros(rows, kp, dtype=dt, device=Ybar.device)
+                P[:, :w] = Tb
+                return P
+            Yb = padded(Ybar, self.nrows)
+            Xin = padded(X, self.ncols) if want_vbar else None
+            Xo = torch.empty(self.ncols, kp, dtype=dt, device=Ybar.device)
+            vout = (vbar if len(blocks) == 1 else part) if want_vbar else None
+            L.check(L.lib().gs_spmm_adjoint(
+                self._h, Yb.data_ptr(), Xin.data_ptr() if Xin is not None else None,
+                Xo.data_ptr(), vout.data_ptr() if vout is not None else None, self.vtype, kp,
+                m, self.ORDERS[order], stream_handle(stream)), "gs_spmm_adjoint")
+            Xbar[:, c0:c0 + w] = Xo[:, :w]
+            if want_vbar and len(blocks) > 1:
+                vbar += part
+        return Xbar, vbar
 
     def device_status(self, reset: bool = True) -> int:
         """Status word of the kernels (bit 0: a bounded wait timed out); synchronises."""

@@ -322,6 +322,46 @@ gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const
                           const double *d_val, const double *d_x, double *d_y,
                           gs_stream stream);
 
+/* ---- multi-RHS products and the adjoint of y = A(v) x (K1 matrices, FP64 or FP32 values,
+ * 32-bit columns).  No counterpart in the reference, which has one right-hand side and no
+ * derivative.  X is row-major [ncols][k], Y row-major [nrows][k], k in {1,2,4,8,16,32},
+ * operands of the matrix's value type and 32-byte aligned. */
+typedef enum {
+    GS_ADJ_DETERMINISTIC = 0, /* transposed K1 layout: fixed summation order, no atomics */
+    GS_ADJ_ATOMIC = 1         /* forward layout with atomic adds into Xbar */
+} gs_adjoint_mode;
+
+/* Order of a value (or value-gradient) array: the CSR order of creation (nnz entries), or
+ * the slot order of the adjoint layout (gs_matrix_value_slots entries, padding slots 0),
+ * in which the deterministic adjoint writes vbar without scattering. */
+typedef enum { GS_VALUES_CSR = 0, GS_VALUES_SLOTS = 1 } gs_value_order;
+
+/* Y = A X.  The first call sizes the matrix's multi-RHS scratch (allocates, synchronises). */
+gs_status gs_spmm(gs_matrix *A, const void *d_X, void *d_Y, gs_dtype dtype, UIN k,
+                  gs_stream stream);
+/* Builds what the adjoint needs from the CSR structure the matrix was created from (the
+ * same d_row / d_col): the map from K1 slots to CSR indices and the K1 layout of A^T with
+ * its values.  Once per matrix; allocates and synchronises. */
+gs_status gs_matrix_prepare_adjoint(gs_matrix *A, const UIN *d_row, const UIN *d_col,
+                                    gs_stream stream);
+/* Replaces the stored values (forward and transposed layouts) by d_val, of the matrix's
+ * value type, in the given order.  Needs the adjoint prepared. */
+gs_status gs_matrix_set_values(gs_matrix *A, const void *d_val, gs_dtype dtype,
+                               gs_value_order order, gs_stream stream);
+/* Number of slots of the adjoint layout (length of a GS_VALUES_SLOTS array). */
+gs_status gs_matrix_value_slots(const gs_matrix *A, UIN *nslots);
+/* Converts a value array between the two orders (CSR -> slots fills padding with 0). */
+gs_status gs_matrix_convert_values(const gs_matrix *A, const void *d_in,
+                                   gs_value_order in_order, void *d_out, gs_dtype dtype,
+                                   gs_stream stream);
+/* Xbar = A^T Ybar (Xbar [ncols][k], overwritten) and, when d_vbar is given,
+ * vbar[e] = sum_r Ybar[row_e][r] * X[col_e][r] for every stored element e, in vbar_order
+ * (the gradient with respect to the values).  The atomic mode needs X and vbar.  X, Ybar
+ * and Xbar are 32-byte aligned. */
+gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, void *d_Xbar,
+                          void *d_vbar, gs_dtype dtype, UIN k, gs_adjoint_mode mode,
+                          gs_value_order vbar_order, gs_stream stream);
+
 /* K1 SpMV that allocates nothing: y[permi[r]] = row r of the K1 layout times x, FP64, from
  * the arrays the reference's gk1 kernel takes (cudaSpmv.cu:851), all on the device, in the
  * str_matK1 layout (chunkNum = ceil(nrows / 32), permi of chunkNum * 32 entries, lenVC
