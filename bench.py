@@ -346,6 +346,61 @@ def time_adjoint(steps: int):
                     "slots = values kept in the adjoint layout's order"}
 
 
+def time_batched(steps: int):
+    """256 banded matrices (rows log-uniform in [1000, 200000], half-bandwidth U[16, 256],
+    U[5, 60] entries per row in the band, FP32 values N(0,1)), each with U[1, 32]
+    right-hand sides N(0,1), seed 3: one persistent launch replayed from a CUDA graph, block
+    widths from the autotuner.  The plain FP64 form is the same work as single-RHS FP64 K1
+    products, one per matrix and right-hand side (device time per product x k_i)."""
+    import torch
+
+    from gpu_spmv_b200 import autotune
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    rng = np.random.default_rng(3)
+    nm = 256
+    nrows = np.exp(rng.uniform(np.log(1000), np.log(200000), nm)).astype(np.int64)
+    hbw = rng.integers(16, 257, nm)
+    ks = [int(k) for k in rng.integers(1, 33, nm)]
+    mats, plain_us, nnz_tot = [], 0.0, 0
+    for i in range(nm):
+        row, col, val = matgen.banded(int(nrows[i]), int(hbw[i]), 5, 60, seed=3000 + i)
+        n = len(row) - 1
+        nnz_tot += len(col)
+        mats.append(E.Matrix(row, col, val, ncols=n, fmt="K1", vtype="f32"))
+        A64 = E.Matrix(row, col, val, ncols=n, fmt="K1")
+        x = torch.randn(n, dtype=torch.float64, device="cuda")
+        y = torch.empty(n, dtype=torch.float64, device="cuda")
+        plain_us += ks[i] * _time_us(lambda: A64.spmv(x, y), 5, warm=2)
+        A64.close()
+    B = E.Batch(mats, ks)
+    g = torch.Generator().manual_seed(3)
+    B.make_operands([torch.randn(A.ncols, k, generator=g) for A, k in zip(mats, ks)])
+    tune = autotune.tune(B, reps=5)
+    us = _time_us(lambda: B.run(graph=True), steps, warm=3)
+    us_default = None
+    kb_tuned = list(B.blocking)
+    B.set_blocking(B.kpad)
+    us_default = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
+    B.set_blocking(kb_tuned)
+    flops = B.flops
+    out = {"workload": "256 banded FP32 matrices, %d rows, %d nnz, 1-32 RHS (sum %d), seed 3"
+                       % (int(nrows.sum()), nnz_tot, sum(ks)),
+           "us_per_run": round(us, 1), "gflops": round(flops / us / 1e3, 1),
+           "us_per_run_untuned": round(us_default, 1),
+           "work_items": B.nitems,
+           "plain_fp64_us": round(plain_us, 1),
+           "plain_fp64_gflops": round(flops / plain_us / 1e3, 1),
+           "speedup_vs_plain_fp64": round(plain_us / us, 2),
+           "autotune": {k: int(v) for k, v in tune["choices"].items()},
+           "autotune_ms": {k: round(v, 3) for k, v in tune["timings"].items()}}
+    B.close()
+    for A in mats:
+        A.close()
+    return out
+
+
 def time_formats(row, col, val, x, steps: int):
     """µs per product of the other formats and of cuSPARSE CSR on the same matrix and x
     (per-launch CUDA events, mean over `steps` launches after warm-up)."""
@@ -578,7 +633,9 @@ def run_ours(args):
                    args.variant: round(1e3 * kern, 2)}
         formats.update(time_formats(row, col, val, x, args.format_steps))
 
-    mixed = adjoint = None
+    mixed = adjoint = batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = time_batched(max(10, args.format_steps // 4))
     if rank == 0 and world == 1 and not args.no_mixed:
         mixed = time_mixed(args.format_steps)
     if rank == 0 and world == 1 and not args.no_adjoint:
@@ -621,6 +678,7 @@ def run_ours(args):
         "formats": formats,
         "mixed": mixed,
         "adjoint": adjoint,
+        "batched": batched,
         "gpu_launches": K,
         "clocks": clocks,
     }
@@ -643,6 +701,7 @@ def main():
     ap.add_argument("--no-formats", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--format-steps", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()

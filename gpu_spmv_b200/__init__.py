@@ -7,12 +7,13 @@ Layers:
   * ``engine``: device-resident matrices (CSR / K1 / AXC / AXT) and SpMV from Python;
   * ``matgen``: seeded synthetic workloads;
   * ``refapi``: ctypes helpers for the drop-in layer;
-  * ``autograd``: Y = A(v) X as a torch.autograd.Function over the hand-written adjoint.
+  * ``autograd``: Y = A(v) X as a torch.autograd.Function over the hand-written adjoint;
+  * ``autotune``: right-hand-side block widths for batched products (``engine.Batch``).
 """
 from . import _lib
 from ._lib import GSError, lib
 
-__all__ = ["GSError", "lib", "engine", "matgen", "refapi", "autograd", "version"]
+__all__ = ["GSError", "lib", "engine", "matgen", "refapi", "autograd", "autotune", "version"]
 
 
 def version() -> str:
@@ -20,7 +21,7 @@ def version() -> str:
 
 
 def __getattr__(name):
-    if name in ("engine", "matgen", "refapi", "autograd"):
+    if name in ("engine", "matgen", "refapi", "autograd", "autotune"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)

@@ -137,6 +137,13 @@ SIGNATURES = {
     "gs_matrix_value_slots": (_st, [_vp, C.POINTER(UIN)]),
     "gs_matrix_convert_values": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, _vp]),
     "gs_spmm_adjoint": (_st, [_vp, _vp, _vp, _vp, _vp, C.c_int, UIN, C.c_int, C.c_int, _vp]),
+    "gs_batch_create": (_st, [C.POINTER(_vp), UIN, C.POINTER(_vp), C.POINTER(UIN), _vp]),
+    "gs_batch_destroy": (_st, [_vp]),
+    "gs_batch_info": (_st, [_vp, C.POINTER(UIN), C.POINTER(UIN), C.POINTER(C.c_double)]),
+    "gs_batch_set_operands": (_st, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
+    "gs_batch_set_blocking": (_st, [_vp, C.POINTER(UIN), _vp]),
+    "gs_batch_run": (_st, [_vp, _vp]),
+    "gs_batch_run_graph": (_st, [_vp, _vp]),
     "gs_copy_to_host": (_st, [_vp, _vp, C.c_size_t]),
     "gs_matrix_device_status": (_st, [_vp, C.POINTER(UIN), C.c_int]),
     "gs_gen_laplacian2d": (_st, [UIN, C.POINTER(UINp), C.POINTER(UINp), C.POINTER(FPTp),

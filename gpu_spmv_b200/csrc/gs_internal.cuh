@@ -219,6 +219,9 @@ gs_status build_k1_plan(const uint32_t *d_nmc, uint32_t chunkNum, DevBuf &unit_c
                         DevBuf &unit_base, DevBuf &partial, DevBuf &count, uint32_t *units,
                         cudaStream_t s);
 
+// Sizes a K1 matrix's multi-RHS scratch once (gs_spmm.cu; allocates, synchronises).
+gs_status prepare_mm_scratch(gs_matrix *A, cudaStream_t s);
+
 // Conversion entry (gs_convert.cu).  x/ax optional: bake x into a reference-layout ax.
 gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t nrows, uint32_t ncols,
                   uint32_t nnz, const uint32_t *d_row, const uint32_t *d_col,

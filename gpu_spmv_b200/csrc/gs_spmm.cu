@@ -20,239 +20,21 @@
 // The reference has no multi-RHS product and no adjoint; these extend its K1 format.
 #include <mutex>
 
-#include "gs_internal.cuh"
+#include "gs_mm.cuh"
 
 namespace gs {
 
 namespace {
 
-constexpr uint32_t kNoSrc = 0xffffffffu;
-
-template <class T> struct Arith;
-template <> struct Arith<double> {
-    __device__ __forceinline__ static double mul(double a, double b) { return __dmul_rn(a, b); }
-    __device__ __forceinline__ static double add(double a, double b) { return __dadd_rn(a, b); }
-};
-template <> struct Arith<float> {
-    __device__ __forceinline__ static float mul(float a, float b) { return __fmul_rn(a, b); }
-    __device__ __forceinline__ static float add(float a, float b) { return __fadd_rn(a, b); }
-};
-
-// 32-byte loads / stores (one request for a 32-byte row; sm_100 256-bit vector access)
-__device__ __forceinline__ void ld32(const float *p, float *v)
-{
-    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
-                   "=f"(v[6]), "=f"(v[7])
-                 : "l"(p));
-}
-__device__ __forceinline__ void ld32(const double *p, double *v)
-{
-    asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
-                 : "l"(p));
-}
-__device__ __forceinline__ void st32(float *p, const float *v)
-{
-    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]),
-                 "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
-                 : "memory");
-}
-__device__ __forceinline__ void st32(double *p, const double *v)
-{
-    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
-                 "d"(v[2]), "d"(v[3])
-                 : "memory");
-}
-
-// K consecutive values of row r of a row-major [*][K] array: 32-byte accesses for rows of
-// 32 bytes or more (base 32-byte aligned), 16-byte ones for 16-byte rows
-template <class T, int K>
-__device__ __forceinline__ void load_row(const T *__restrict__ X, uint32_t r, T (&v)[K])
-{
-    const T *p = X + (size_t)r * K;
-    if constexpr (sizeof(T) * K >= 32) {
-        constexpr int per = 32 / (int)sizeof(T);
-#pragma unroll
-        for (int i = 0; i < K / per; i++) ld32(p + i * per, v + i * per);
-    } else if constexpr (sizeof(T) * K >= 16) {
-        constexpr int per = 16 / (int)sizeof(T);
-#pragma unroll
-        for (int i = 0; i < K / per; i++) {
-            if constexpr (sizeof(T) == 8) {
-                const double2 w = __ldg(reinterpret_cast<const double2 *>(p) + i);
-                v[2 * i] = w.x;
-                v[2 * i + 1] = w.y;
-            } else {
-                const float4 w = __ldg(reinterpret_cast<const float4 *>(p) + i);
-                v[4 * i] = w.x;
-                v[4 * i + 1] = w.y;
-                v[4 * i + 2] = w.z;
-                v[4 * i + 3] = w.w;
-            }
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < K; k++) v[k] = __ldg(p + k);
-    }
-}
-
-template <class T, int K>
-__device__ __forceinline__ void store_row(T *__restrict__ Y, uint32_t r, const T (&v)[K])
-{
-    T *p = Y + (size_t)r * K;
-    if constexpr (sizeof(T) * K >= 32) {
-        constexpr int per = 32 / (int)sizeof(T);
-#pragma unroll
-        for (int i = 0; i < K / per; i++) st32(p + i * per, v + i * per);
-    } else if constexpr (sizeof(T) * K >= 16) {
-        constexpr int per = 16 / (int)sizeof(T);
-#pragma unroll
-        for (int i = 0; i < K / per; i++) {
-            if constexpr (sizeof(T) == 8)
-                reinterpret_cast<double2 *>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
-            else
-                reinterpret_cast<float4 *>(p)[i] =
-                    make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < K; k++) p[k] = v[k];
-    }
-}
-
-// slots in flight per lane: at most 8, and at most 128 bytes of gathered rows (more
-// registers would cost occupancy, which the latency-bound gathers need more)
-template <class T, int K> constexpr int mm_batch()
-{
-    return (128 / (K * (int)sizeof(T))) < 1 ? 1
-           : ((128 / (K * (int)sizeof(T))) > 8 ? 8 : 128 / (K * (int)sizeof(T)));
-}
-
-struct MMArgs {
-    uint32_t nrows;                            // rows of this layout (A: n, A^T: ncols)
-    const uint32_t *permi, *nmc, *chp, *klen;  // K1 layout
-    const void *val;
-    const uint32_t *col;                       // gathered row index (A: col, A^T: row of A)
-    const uint32_t *src;                       // A^T only: CSR index of each slot
-    const void *xin;                           // gathered operand (A: X, A^T: Ybar)
-    const void *xrow;                          // A^T only: X, row j held for vbar
-    void *yout;                                // A: Y, A^T: Xbar
-    void *vbar;                                // A^T only, or nullptr
-    bool vbar_slots;                           // vbar in this layout's slot order
-    const uint32_t *unit_chunk, *unit_base;
-    uint32_t units, split_units;               // units < split_units may be pieces
-    void *partial;                             // split_units * 32 * K values
-    uint32_t *count;
-};
+using namespace mm;
 
 template <class T, int K, bool ADJ>
 __global__ void __launch_bounds__(256) k_k1_mm(const MMArgs a)
 {
-    using A = Arith<T>;
-    constexpr int B = mm_batch<T, K>();
-    const T *__restrict__ val = static_cast<const T *>(a.val);
-    const T *__restrict__ xin = static_cast<const T *>(a.xin);
-    T *__restrict__ yout = static_cast<T *>(a.yout);
-    T *__restrict__ partial = static_cast<T *>(a.partial);
-    const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
-         u += warps) {
-        const uint32_t c = __ldg(a.unit_chunk + u);
-        const uint32_t ub = __ldg(a.unit_base + c);
-        const uint32_t np = __ldg(a.unit_base + c + 1) - ub;
-        const uint32_t piece = u - ub;
-        const uint32_t g = 32u * c + (uint32_t)lane;
-        const bool valid = g < a.nrows;
-        const uint32_t len = valid ? __ldg(a.klen + g) : 0u;
-        const uint32_t j0 = piece * kK1Split;
-        const uint32_t j1 = min(len, j0 + kK1Split);
-        const uint32_t base = __ldg(a.chp + c) + (uint32_t)lane;
-        const uint32_t me = valid ? __ldg(a.permi + g) : 0u;
-        T xr[K];
-        if constexpr (ADJ) {
-            if (a.vbar && j0 < j1) load_row<T, K>(static_cast<const T *>(a.xrow), me, xr);
-        }
-        T acc[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) acc[k] = T(0);
-        for (uint32_t j = j0; j < j1; j += B) {
-            T v[B], gv[B][K];
-            uint32_t cc[B], sr[B];
-#pragma unroll
-            for (int b = 0; b < B; b++) {
-                const bool in = j + b < j1;
-                const uint32_t pos = base + 32u * (j + b);
-                v[b] = in ? __ldcs(val + pos) : T(0);
-                cc[b] = in ? __ldcs(a.col + pos) : 0u;
-                if constexpr (ADJ)
-                    sr[b] = (in && a.vbar && !a.vbar_slots) ? __ldcs(a.src + pos) : kNoSrc;
-            }
-#pragma unroll
-            for (int b = 0; b < B; b++) {
-                if (j + b < j1) load_row<T, K>(xin, cc[b], gv[b]);
-                else {
-#pragma unroll
-                    for (int k = 0; k < K; k++) gv[b][k] = T(0);
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < B; b++) {
-                if (j + b < j1) {
-#pragma unroll
-                    for (int k = 0; k < K; k++) acc[k] = A::add(acc[k], A::mul(v[b], gv[b][k]));
-                }
-            }
-            if constexpr (ADJ) {
-                if (a.vbar) {
-#pragma unroll
-                    for (int b = 0; b < B; b++) {
-                        if (j + b < j1) {
-                            T d = T(0);
-#pragma unroll
-                            for (int k = 0; k < K; k++) d = A::add(d, A::mul(gv[b][k], xr[k]));
-                            static_cast<T *>(a.vbar)[a.vbar_slots ? base + 32u * (j + b)
-                                                                  : sr[b]] = d;
-                        }
-                    }
-                }
-            }
-        }
-        if constexpr (ADJ) {
-            // slot order: this piece's padding slots of the lane get a zero gradient
-            if (a.vbar && a.vbar_slots) {
-                const uint32_t pend = min(__ldg(a.nmc + c), j0 + kK1Split);
-                for (uint32_t j = max(j0, len); j < pend; j++)
-                    static_cast<T *>(a.vbar)[base + 32u * j] = T(0);
-            }
-        }
-        if (np == 1) {
-            if (valid) store_row<T, K>(yout, me, acc);
-            continue;
-        }
-        // split chunk: the pieces of chunk c are units ub .. ub+np-1 < split_units
-#pragma unroll
-        for (int k = 0; k < K; k++) partial[((size_t)u * K + k) * 32 + lane] = acc[k];
-        __threadfence();
-        __syncwarp();
-        uint32_t ticket = 0;
-        if (lane == 0) ticket = atomicAdd(a.count + c, 1u);
-        ticket = __shfl_sync(0xffffffffu, ticket, 0);
-        if (ticket == np - 1) {
-            __threadfence();
-            T s[K];
-#pragma unroll
-            for (int k = 0; k < K; k++) s[k] = T(0);
-            for (uint32_t q = 0; q < np; q++) {
-#pragma unroll
-                for (int k = 0; k < K; k++)
-                    s[k] = A::add(s[k], __ldcg(partial + ((size_t)(ub + q) * K + k) * 32 + lane));
-            }
-            if (valid) store_row<T, K>(yout, me, s);
-            if (lane == 0) a.count[c] = 0;
-        }
-    }
+         u += warps)
+        mm_unit<T, K, ADJ>(a, u, 0);
 }
 
 // Atomic-mode adjoint on the forward layout, over the same 256-step work units: lane = row
@@ -302,7 +84,7 @@ __global__ void __launch_bounds__(256) k_k1_adj_atomic(const AtomicArgs a)
         const uint32_t j1 = min(len, j0 + kK1Split);
         if (j0 >= j1) continue;
         T yb[K];
-        load_row<T, K>(static_cast<const T *>(a.ybar), __ldg(a.permi + g), yb);
+        load_row<T, K>(static_cast<const T *>(a.ybar), __ldg(a.permi + g), K, yb);
         const uint32_t base = __ldg(a.chp + c) + (uint32_t)lane;
         for (uint32_t j = j0; j < j1; j += B) {
             T v[B], xg[B][K];
@@ -317,7 +99,7 @@ __global__ void __launch_bounds__(256) k_k1_adj_atomic(const AtomicArgs a)
             }
 #pragma unroll
             for (int b = 0; b < B; b++) {
-                if (j + b < j1) load_row<T, K>(x, cc[b], xg[b]);
+                if (j + b < j1) load_row<T, K>(x, cc[b], K, xg[b]);
             }
 #pragma unroll
             for (int b = 0; b < B; b++) {
@@ -542,6 +324,8 @@ void refresh_values(gs_matrix *A, const T *v, gs_value_order order, cudaStream_t
 
 }  // namespace
 
+gs_status prepare_mm_scratch(gs_matrix *A, cudaStream_t s) { return ensure_mm_scratch(A, s); }
+
 }  // namespace gs
 
 using namespace gs;
@@ -574,6 +358,8 @@ gs_status gs_spmm(gs_matrix *A, const void *d_X, void *d_Y, gs_dtype dtype, UIN 
     a.split_units = A->k1split_units;
     a.partial = A->mmpartial.p;
     a.count = A->k1count.as<uint32_t>();
+    a.ld = k;
+    a.nrb = 1;
     if (A->p.vtype == GS_F64) return launch_mm<double, false>(a, k, s);
     return launch_mm<float, false>(a, k, s);
 }
@@ -810,6 +596,8 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
     a.split_units = A->tsplit_units;
     a.partial = A->tpartial.p;
     a.count = A->tcount.as<uint32_t>();
+    a.ld = k;
+    a.nrb = 1;
     return f64 ? launch_mm<double, true>(a, k, s) : launch_mm<float, true>(a, k, s);
 }
 

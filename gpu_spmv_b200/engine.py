@@ -297,3 +297,85 @@ def csr_spmv_f64(row: torch.Tensor, col: torch.Tensor, val: torch.Tensor, x: tor
 
 def algorithmic_bytes(nrows, ncols, nnz, k=1, s_v=8, s_i=4, s_x=8, s_y=8) -> float:
     return L.lib().gs_algorithmic_bytes(nrows, ncols, nnz, k, s_v, s_i, s_x, s_y)
+
+
+class Batch:
+    """Y_i = A_i X_i for many K1 matrices (FP64 or FP32) in one persistent launch.
+
+    mats: K1 Matrix objects of one value type; ks: right-hand sides per matrix (1..32).
+    Operands are [ncols_i, kpad_i] / [nrows_i, kpad_i] tensors (kpad_i = next power of two
+    >= k_i; make_operands builds them, zero in the padding columns).
+    """
+
+    def __init__(self, mats, ks, stream=None):
+        self.mats = list(mats)
+        self.ks = [int(k) for k in ks]
+        n = len(self.mats)
+        arr_m = (C.c_void_p * max(1, n))(*[m._h for m in self.mats])
+        arr_k = (L.UIN * max(1, n))(*self.ks)
+        h = C.c_void_p()
+        L.check(L.lib().gs_batch_create(C.byref(h), n, arr_m, arr_k, stream_handle(stream)),
+                "gs_batch_create")
+        self._h = h
+        kp = (L.UIN * max(1, n))()
+        nitems = L.UIN()
+        flops = C.c_double()
+        L.check(L.lib().gs_batch_info(h, C.byref(nitems), kp, C.byref(flops)), "gs_batch_info")
+        self.kpad = [int(kp[i]) for i in range(n)]
+        self.flops = flops.value
+        self.blocking = list(self.kpad)
+        self.dtype = TORCH_DTYPES[self.mats[0].vtype] if n else torch.float64
+        self.X = self.Y = None
+
+    @property
+    def nitems(self) -> int:
+        v = L.UIN()
+        L.check(L.lib().gs_batch_info(self._h, C.byref(v), None, None), "gs_batch_info")
+        return v.value
+
+    def make_operands(self, Xs):
+        """Padded device copies of the right-hand sides Xs[i] ([ncols_i, k_i]) and output
+        buffers; registers them with the batch and returns (X list, Y list)."""
+        dev = torch.device("cuda")
+        X, Y = [], []
+        for A, kp, k, x in zip(self.mats, self.kpad, self.ks, Xs):
+            xp = torch.zeros(A.ncols, kp, dtype=self.dtype, device=dev)
+            xp[:, :k] = torch.as_tensor(x, dtype=self.dtype).reshape(A.ncols, k).to(dev)
+            X.append(xp)
+            Y.append(torch.empty(A.nrows, kp, dtype=self.dtype, device=dev))
+        self.set_operands(X, Y)
+        return X, Y
+
+    def set_operands(self, X, Y, stream=None):
+        n = len(self.mats)
+        ax = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in X])
+        ay = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in Y])
+        L.check(L.lib().gs_batch_set_operands(self._h, ax, ay, stream_handle(stream)),
+                "gs_batch_set_operands")
+        self.X, self.Y = X, Y
+
+    def set_blocking(self, kb, stream=None):
+        n = len(self.mats)
+        arr = (L.UIN * max(1, n))(*[int(b) for b in kb])
+        L.check(L.lib().gs_batch_set_blocking(self._h, arr, stream_handle(stream)),
+                "gs_batch_set_blocking")
+        self.blocking = [int(b) for b in kb]
+
+    def run(self, graph: bool = True, stream=None):
+        f = L.lib().gs_batch_run_graph if graph else L.lib().gs_batch_run
+        L.check(f(self._h, stream_handle(stream)), "gs_batch_run")
+
+    def results(self):
+        """Y_i[:, :k_i] views."""
+        return [y[:, :k] for y, k in zip(self.Y, self.ks)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().gs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -362,6 +362,33 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
                           void *d_vbar, gs_dtype dtype, UIN k, gs_adjoint_mode mode,
                           gs_value_order vbar_order, gs_stream stream);
 
+/* ---- batched uneven multi-RHS products: Y_i = A_i X_i for many K1 matrices in one
+ * persistent launch (no counterpart in the reference).  All matrices share one value type
+ * (FP64 or FP32, 32-bit columns); matrix i has k_i right-hand sides (1..32), stored padded
+ * to kpad_i = the next power of two: X_i row-major [ncols_i][kpad_i], Y_i [nrows_i][kpad_i],
+ * 32-byte aligned (the padding columns of Y_i receive A_i times the padding of X_i). */
+typedef struct gs_batch gs_batch;
+/* Builds the work list (matrix, K1 unit, right-hand-side block), longest first; allocates
+ * and synchronises.  Each matrix starts with one block of kpad_i columns. */
+gs_status gs_batch_create(gs_batch **out, UIN count, gs_matrix *const *mats, const UIN *k,
+                          gs_stream stream);
+gs_status gs_batch_destroy(gs_batch *B);
+/* Number of work items, each matrix's kpad (array of count, optional) and the batch's
+ * FLOPs per run (2 sum nnz_i k_i). */
+gs_status gs_batch_info(const gs_batch *B, UIN *nitems, UIN *kpad, double *flops);
+/* Device pointers of every X_i and Y_i (host arrays of count pointers); synchronises.
+ * Replaces the operands without invalidating a captured graph. */
+gs_status gs_batch_set_operands(gs_batch *B, void *const *d_X, void *const *d_Y,
+                                gs_stream stream);
+/* Right-hand-side block width of each matrix (a power of two dividing kpad_i): kpad_i/kb_i
+ * passes over A_i, each gathering kb_i values per stored element.  Rebuilds the work list
+ * (and drops a captured graph). */
+gs_status gs_batch_set_blocking(gs_batch *B, const UIN *kb, gs_stream stream);
+/* One run: a counter reset and one persistent kernel launch on `stream`. */
+gs_status gs_batch_run(gs_batch *B, gs_stream stream);
+/* The same run replayed from a CUDA graph captured on the first call. */
+gs_status gs_batch_run_graph(gs_batch *B, gs_stream stream);
+
 /* K1 SpMV that allocates nothing: y[permi[r]] = row r of the K1 layout times x, FP64, from
  * the arrays the reference's gk1 kernel takes (cudaSpmv.cu:851), all on the device, in the
  * str_matK1 layout (chunkNum = ceil(nrows / 32), permi of chunkNum * 32 entries, lenVC

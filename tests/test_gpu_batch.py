@@ -1,0 +1,117 @@
+"""Batched uneven multi-RHS products (gs_batch_*): one persistent launch over many K1
+matrices.  Every column of every matrix sums its products in the same order as the
+single-matrix product, whatever the right-hand-side blocking, so results are compared bit
+for bit with Matrix.spmm; CUDA-graph replays see new operands without a new capture."""
+import numpy as np
+import pytest
+import torch
+
+from mats import case
+
+pytestmark = pytest.mark.gpu
+
+
+def _mats(dtype, rng, count=10):
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    names = ["mixed", "row0_empty", "dense_row", "k1_empty_chunk", "single_row",
+             "powerlaw_small", "laplacian"]
+    out = []
+    for i in range(count):
+        if i < len(names):
+            row, col, val = case(names[i], rng)
+        else:
+            n = int(rng.integers(1000, 20000))
+            row, col, val = matgen.banded(n, int(rng.integers(16, 257)), 5, 60,
+                                          seed=int(rng.integers(1 << 30)))
+        n = len(row) - 1
+        ncols = max(n, int(col.max()) + 1 if len(col) else n)
+        out.append(E.Matrix(row, col, val, ncols=ncols, fmt="K1", vtype=dtype))
+    return out
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_batch_equals_single_products(dtype):
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(3)
+    mats = _mats(dtype, rng)
+    ks = [int(k) for k in rng.integers(1, 33, len(mats))]
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    B = E.Batch(mats, ks)
+    assert B.kpad == [1 << (k - 1).bit_length() for k in ks]
+    Xs = [rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)]
+    X, Y = B.make_operands(Xs)
+    ref = [A.spmm(x) for A, x in zip(mats, X)]
+    B.run(graph=False)
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, r)
+    # any blocking: the same sums in the same order
+    B.set_blocking([max(1, kp // 4) for kp in B.kpad])
+    for y in Y:
+        y.fill_(float("nan"))
+    B.run(graph=True)
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, r)
+    # new right-hand sides, same captured graph
+    for x in X:
+        x.mul_(-2.0)
+    B.run(graph=True)
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, -2.0 * r)
+    assert all(r.dtype == tdt for r in ref)
+    B.close()
+
+
+def test_autotune_keeps_results(tmp_path):
+    from gpu_spmv_b200 import autotune
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(5)
+    mats = _mats("f32", rng, count=12)
+    ks = [32, 17, 8, 3, 1, 32, 24, 9, 16, 5, 2, 31]
+    B = E.Batch(mats, ks)
+    X, Y = B.make_operands([rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)])
+    B.run(graph=False)
+    torch.cuda.synchronize()
+    before = [y.clone() for y in Y]
+    cache = tmp_path / "tune.json"
+    info = autotune.tune(B, reps=3, cache_path=str(cache))
+    assert cache.exists() and info["choices"]
+    assert all(kp % kb == 0 for kp, kb in zip(B.kpad, B.blocking))
+    B.run(graph=True)
+    torch.cuda.synchronize()
+    for y, r in zip(Y, before):
+        assert torch.equal(y, r)
+    # cached choices are reused without timing
+    info2 = autotune.tune(B, reps=3, cache_path=str(cache))
+    assert info2["choices"] == info["choices"] and not info2["timings"]
+    B.close()
+
+
+def test_batch_argument_errors():
+    from gpu_spmv_b200 import GSError
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(1)
+    row, col, val = case("mixed", rng)
+    n = len(row) - 1
+    a64 = E.Matrix(row, col, val, ncols=n, fmt="K1")
+    a32 = E.Matrix(row, col, val, ncols=n, fmt="K1", vtype="f32")
+    csr = E.Matrix(row, col, val, ncols=n, fmt="CSR")
+    with pytest.raises(GSError, match="share one value type"):
+        E.Batch([a64, a32], [1, 1])
+    with pytest.raises(GSError, match="K1 matrices"):
+        E.Batch([csr], [1])
+    with pytest.raises(GSError, match="right-hand sides"):
+        E.Batch([a64], [33])
+    B = E.Batch([a64], [8])
+    with pytest.raises(GSError, match="set_operands"):
+        B.run()
+    with pytest.raises(GSError, match="power of two"):
+        B.set_blocking([3])
+    B.close()
