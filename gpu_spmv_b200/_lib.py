@@ -70,6 +70,35 @@ class StrMatAXT(C.Structure):  # cudaSpmv.cu:1154
                 ("ax", FPTp), ("sec", UINp), ("con", UINp)]
 
 
+# ------------------------------------------------------------------ second API generation
+class Gen2MatCSR(C.Structure):  # gpuSpmv_header.h:252
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("rmin", UIN), ("rave", FPT), ("rmax", UIN),
+                ("rsd", FPT), ("bw", UIN), ("val", FPTp), ("row", UINp), ("col", UINp),
+                ("rl", UINp)]
+
+
+class Gen2FormatData(C.Structure):  # gpuSpmv_header.h:375
+    _fields_ = [("name", C.c_char * 18), ("mfp", C.c_double), ("beta", C.c_double),
+                ("ct", C.c_double)]
+
+
+class Gen2Res(C.Structure):  # gpuSpmv_header.h:469
+    _fields_ = [("name", C.c_char * 24), ("et", C.c_double), ("flops", C.c_double),
+                ("sErr", StrErr)]
+
+
+class Gen2MatAXC(C.Structure):  # gpuSpmv_header.h:675
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("lenAX", UIN), ("lenBRP", UIN), ("ax", FPTp),
+                ("brp", UINp)]
+
+
+class Gen2MatAXT(C.Structure):  # gpuSpmv_header.h:1082
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("mode", C.c_char * 8), ("tileHW", UIN),
+                ("tileH", UIN), ("logTH", UIN), ("tileN", UIN), ("lenAX", UIN),
+                ("lenSEC", UIN), ("lenCON", UIN), ("log", UIN), ("ax", FPTp), ("sec", UINp),
+                ("con", UINp)]
+
+
 # ------------------------------------------------------------------ native structs
 class ConvertParams(C.Structure):
     _fields_ = [("format", C.c_int), ("tileHW", UIN), ("tileH", UIN), ("bs", UIN),
@@ -116,6 +145,25 @@ SIGNATURES = {
     "test_gaxtuh": (StrRes, [UIN, UIN, StrMatAXT, FPTp]),
     "test_gaxtch1": (StrRes, [UIN, StrMatAXT, FPTp]),
     "test_gaxtch": (StrRes, [UIN, StrMatAXT, FPTp]),
+    # second API generation (gpuspmv_b200_gen2.h)
+    "gs2_matrixReading": (Gen2MatCSR, [C.c_char_p]),
+    "gs2_printMatrixStats": (None, [C.c_char_p, C.POINTER(Gen2MatCSR)]),
+    "gs2_getFormatDataCSR": (Gen2FormatData, [Gen2MatCSR]),
+    "gs2_initVec": (None, [UIN, FPTp]),
+    "gs2_cf_CSR": (None, [Gen2MatCSR, FPTp, FPTp]),
+    "gs2_getErrors": (None, [UIN, FPTp, FPTp, C.POINTER(StrErr)]),
+    "gs2_test_cf_CSR": (Gen2Res, [Gen2MatCSR, FPTp, FPTp]),
+    "gs2_test_gk_CSR": (Gen2Res, [UIN, Gen2MatCSR, FPTp, FPTp]),
+    "gs2_test_gcu_CSR": (Gen2Res, [Gen2MatCSR, FPTp, FPTp]),
+    "gs2_getFormatDataAXC": (Gen2FormatData, [UIN, Gen2MatCSR, FPTp, C.POINTER(Gen2MatAXC)]),
+    "gs2_test_gk_AXC": (Gen2Res, [UIN, Gen2MatAXC, FPTp]),
+    "gs2_getFormatDataK1": (Gen2FormatData, [UIN, Gen2MatCSR, FPTp, C.POINTER(StrMatK1)]),
+    "gs2_test_gk_K1": (Gen2Res, [UIN, StrMatK1, FPTp, FPTp]),
+    "gs2_getFormatDataAXT": (Gen2FormatData, [UIN, UIN, UIN, UIN, C.c_char_p, Gen2MatCSR, FPTp,
+                                              C.POINTER(Gen2MatAXT)]),
+    "gs2_test_gk_AXT_NOC_H1": (Gen2Res, [UIN, Gen2MatAXT, FPTp]),
+    "gs2_test_gk_AXT_NOC": (Gen2Res, [UIN, Gen2MatAXT, FPTp]),
+    "gs2_test_gk_AXT_COM_H1": (Gen2Res, [UIN, Gen2MatAXT, FPTp]),
     # native layer
     "gs_status_string": (C.c_char_p, [_st]),
     "gs_last_error": (C.c_char_p, []),

@@ -14,11 +14,13 @@
 //    counts -- gaxtch1 drops it (cudaSpmv.cu:2089).
 #include <cusparse.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <vector>
 
 #include "gs_internal.cuh"
 
@@ -249,7 +251,12 @@ int matrixWritingBin(const char *matFileName, const str_matCSR *m)
     return (fclose(fh) == 0 && ok) ? 0 : -1;
 }
 
-void printMatrixStats(const char *matFileName, str_matCSR *m)
+}  // extern "C"
+
+// Statistics of cudaSpmv.cu:332-381 (and gpuSpmv_header.h:322-371, the same numbers and
+// file) written to "<name>.sta": name = the path up to the first '.' of its last component
+// (first API generation) or of the whole path (second: strtok on the full name).
+static void stats_core(const char *matFileName, str_matCSR *m, bool dot_anywhere)
 {
     UIN rmin = 1000000000u, rmax = 0, bw = 0;
     double s1 = 0.0, s2 = 0.0;
@@ -276,7 +283,7 @@ void printMatrixStats(const char *matFileName, str_matCSR *m)
     // "<file name up to its first '.'>.sta", next to the matrix file
     char path[512];
     snprintf(path, sizeof(path), "%s", matFileName ? matFileName : "matrix");
-    char *slash = strrchr(path, '/');
+    char *slash = dot_anywhere ? nullptr : strrchr(path, '/');
     char *dot = strchr(slash ? slash + 1 : path, '.');
     if (dot) *dot = 0;
     strncat(path, ".sta", sizeof(path) - strlen(path) - 1);
@@ -296,6 +303,10 @@ void printMatrixStats(const char *matFileName, str_matCSR *m)
     fprintf(fh, "bw:    %28d\n", m->bw);
     fclose(fh);
 }
+
+extern "C" {
+
+void printMatrixStats(const char *matFileName, str_matCSR *m) { stats_core(matFileName, m, false); }
 
 str_formatData getFormatDataCSR(str_matCSR *m)
 {
@@ -692,6 +703,367 @@ str_res test_gaxtch(const UIN cudaBlockSize, const str_matAXT m, const FPT *ref)
     snprintf(name, sizeof(name), "gaxtch%u", m.tileH);
     if (m.tileH < 2) return error_res(name, "tileH must be > 1");
     return test_com(name, m, ref);
+}
+
+}  // extern "C"
+
+// ======================================================================================
+// Second API generation (gpuSpmv_header.h), exported as gs2_* (gpuspmv_b200_gen2.h).
+// Each call maps the second generation's structs onto the first generation's and reuses its
+// converters and entry points; only the arrays that differ are made here: COM tileH = 1
+// header words at every tile boundary and con for every row (gpuSpmv_header.h:1086-1115,
+// 1193-1227).
+// ======================================================================================
+#define GS2_NO_ALIASES
+#include "gpuspmv_b200_gen2.h"
+
+namespace {
+
+// con[r] = ax position of the start of row r (gpuSpmv_header.h:1097-1101 with positions =
+// row length, COM); COM tileH = 1 (sec != nullptr): header word at every element that
+// starts a row or a tile, (row << log) | min(elements left in the row - 1, 31 - p % thw)
+// with the reference's unsigned arithmetic.
+__global__ void k_gen2_com(UIN n, const UIN *row, UIN thw, UIN th, UIN log, UIN *sec,
+                           UIN *con)
+{
+    const UIN r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const UIN ths = thw * th, p0 = row[r];
+    const UIN t = (p0 + ths) / ths - 1;
+    con[r] = t * (2 * ths) + (p0 % th) * (2 * thw) + ((p0 + th) / th - 1 - t * thw);
+    if (!sec) return;
+    const UIN len = row[r + 1] - p0;
+    for (UIN e = 0; e < len; e++) {
+        const UIN p = p0 + e, c = p % thw;
+        if (c == 0 || e == 0) {
+            const UIN q1 = len - e - 1, q2 = 31u - c;
+            sec[p] = (r << log) | (q1 > q2 ? q2 : q1);
+        }
+    }
+}
+
+// rpos[r] = CSR position of row r's first element from con (COM tileH = 1), rpos[n] = nnz
+__global__ void k_gen2_com_rpos(UIN n, UIN nnz, const UIN *con, UIN thw, UIN *rpos)
+{
+    const UIN r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) rpos[r] = (con[r] / (2 * thw)) * thw + con[r] % (2 * thw);
+    if (r == n) rpos[n] = nnz;
+}
+
+str_matCSR gen1_view(const gs2_matCSR &m)
+{
+    str_matCSR v;
+    memset(&v, 0, sizeof(v));
+    strcpy(v.name, "gen2");
+    v.nrows = m.nrows;
+    v.nnz = m.nnz;
+    v.rmin = m.rmin;
+    v.rave = m.rave;
+    v.rmax = m.rmax;
+    v.rsd = m.rsd;
+    v.bw = m.bw;
+    v.val = m.val;
+    v.row = m.row;
+    v.col = m.col;
+    v.rl = m.rl;
+    return v;
+}
+
+gs2_res gen2_res(const str_res &r, const char *name)
+{
+    gs2_res o;
+    memset(&o, 0, sizeof(o));
+    snprintf(o.name, sizeof(o.name), "%s", strcmp(r.name, "error") ? name : "error");
+    o.et = r.et;
+    o.flops = r.flops;
+    o.sErr.aErr = r.sErr.aErr;
+    o.sErr.rErr = r.sErr.rErr;
+    o.sErr.pos = r.sErr.pos;
+    return o;
+}
+
+gs2_formatData gen2_fd(const char *name, double mfp, double beta, double ct)
+{
+    gs2_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    const size_t len = std::min(strlen(name), sizeof(fd.name) - 1);  // name[18]
+    memcpy(fd.name, name, len);
+    fd.mfp = mfp;
+    fd.beta = beta;
+    fd.ct = ct;
+    return fd;
+}
+
+gs2_formatData gen2_error_fd()
+{
+    gs2_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    strcpy(fd.name, "error");
+    return fd;
+}
+
+// first-generation view of a second-generation AXT with con[n] appended (lenCON = n here,
+// n + 1 entries there); `ext` owns the copy
+str_matAXT gen1_axt(const gs2_matAXT &m, const char *mode, std::vector<UIN> &ext)
+{
+    str_matAXT v;
+    memset(&v, 0, sizeof(v));
+    strcpy(v.name, "gen2");
+    v.nrows = m.nrows;
+    v.nnz = m.nnz;
+    snprintf(v.mode, sizeof(v.mode), "%s", mode);
+    v.tileHW = m.tileHW;
+    v.tileH = m.tileH;
+    v.logTH = m.logTH;
+    v.tileN = m.tileN;
+    v.lenAX = m.lenAX;
+    v.lenSEC = m.lenSEC;
+    v.lenCON = m.lenCON;
+    v.log = m.log;
+    v.bs = 1u << m.log;
+    v.ax = m.ax;
+    v.sec = m.sec;
+    ext.assign(m.con, m.con + m.lenCON);
+    ext.push_back(m.lenAX);
+    v.con = ext.data();
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+gs2_matCSR gs2_matrixReading(const char *matFileName)
+{
+    const str_matCSR r = matrixReading(matFileName);
+    gs2_matCSR m;
+    memset(&m, 0, sizeof(m));
+    m.nrows = r.nrows;
+    m.nnz = r.nnz;
+    m.val = r.val;
+    m.row = r.row;
+    m.col = r.col;
+    m.rl = r.rl;
+    return m;
+}
+
+void gs2_printMatrixStats(const char *matFileName, gs2_matCSR *m)
+{
+    str_matCSR v = gen1_view(*m);
+    stats_core(matFileName, &v, true);
+    m->rmin = v.rmin;
+    m->rave = v.rave;
+    m->rmax = v.rmax;
+    m->rsd = v.rsd;
+    m->bw = v.bw;
+}
+
+gs2_formatData gs2_getFormatDataCSR(const gs2_matCSR m)
+{
+    return gen2_fd("CSR",
+                   (double)m.nnz * sizeof(FPT) + (double)m.nnz * sizeof(UIN) +
+                       ((double)m.nrows + 1) * sizeof(UIN) + (double)m.nrows * sizeof(FPT),
+                   (double)m.nnz / (double)m.nnz, 0.0);
+}
+
+void gs2_initVec(const UIN len, FPT *vec) { init_vec(1, len, vec); }
+
+void gs2_cf_CSR(const gs2_matCSR m, const FPT *vec, FPT *res) { ncsr(1, gen1_view(m), vec, res); }
+
+void gs2_getErrors(const UIN len, const FPT *ar, const FPT *ac, gs2_err *e)
+{
+    str_err r;
+    get_errors(len, ar, ac, &r);
+    e->aErr = r.aErr;
+    e->rErr = r.rErr;
+    e->pos = r.pos;
+}
+
+gs2_res gs2_test_cf_CSR(const gs2_matCSR m, const FPT *vec, const FPT *ref)
+{
+    return gen2_res(test_gcsr(0, gen1_view(m), vec, ref), "cf_CSR");
+}
+
+gs2_res gs2_test_gk_CSR(const UIN cudaBlockSize, const gs2_matCSR m, const FPT *vec,
+                        const FPT *ref)
+{
+    return gen2_res(test_gcsr(cudaBlockSize, gen1_view(m), vec, ref), "gk_CSR");
+}
+
+gs2_res gs2_test_gcu_CSR(const gs2_matCSR m, const FPT *vec, const FPT *ref)
+{
+    return gen2_res(test_gcucsr(gen1_view(m), vec, ref), "gcu_CSR");
+}
+
+gs2_formatData gs2_getFormatDataAXC(const UIN ompNumThreads, const gs2_matCSR m,
+                                    const FPT *vec, gs2_matAXC *a)
+{
+    str_matAXC a1;
+    memset(&a1, 0, sizeof(a1));
+    const str_formatData fd = getFormatDataAXC(ompNumThreads, 32, gen1_view(m), vec, &a1);
+    if (!strcmp(fd.name, "error")) return gen2_error_fd();
+    free(a1.mapx);
+    a->nrows = a1.nrows;
+    a->nnz = a1.nnz;
+    a->lenAX = a1.lenAX;
+    a->lenBRP = a1.lenBRP;
+    a->ax = a1.ax;
+    a->brp = a1.brp;
+    return gen2_fd("AXC", (double)a->lenAX * sizeof(FPT) + (double)a->lenBRP * sizeof(UIN),
+                   (double)a->nnz / (double)(a->lenAX >> 1), fd.ct);
+}
+
+gs2_res gs2_test_gk_AXC(const UIN cudaBlockSize, const gs2_matAXC a, const FPT *ref)
+{
+    str_matAXC v;
+    memset(&v, 0, sizeof(v));
+    v.nrows = a.nrows;
+    v.nnz = a.nnz;
+    v.hbs = 32;
+    v.lenAX = a.lenAX;
+    v.lenBRP = a.lenBRP;
+    v.ax = a.ax;
+    v.brp = a.brp;
+    return gen2_res(test_gaxc(cudaBlockSize, v, ref), "gk_AXC");
+}
+
+gs2_formatData gs2_getFormatDataK1(const UIN cudaBlockSize, const gs2_matCSR m, const FPT *vec,
+                                   gs2_matK1 *k)
+{
+    str_matK1 k1;
+    memset(&k1, 0, sizeof(k1));
+    const str_formatData fd = getFormatDataK1(cudaBlockSize, gen1_view(m), vec, &k1);
+    if (!strcmp(fd.name, "error")) return gen2_error_fd();
+    static_assert(sizeof(str_matK1) == sizeof(gs2_matK1), "K1 structs of both generations");
+    memcpy(k, &k1, sizeof(k1));
+    return gen2_fd("K1",
+                   (double)k->chunkNum * sizeof(UIN) * 2 + (double)k->lenVC * sizeof(FPT) +
+                       (double)k->lenVC * sizeof(UIN) + (double)k->chunkNum * 32 * sizeof(UIN) +
+                       (double)k->nrows * sizeof(FPT),
+                   (double)k->nnz / (double)k->lenVC, fd.ct);
+}
+
+gs2_res gs2_test_gk_K1(const UIN cudaBlockSize, const gs2_matK1 k, const FPT *vec,
+                       const FPT *ref)
+{
+    str_matK1 k1;
+    memcpy(&k1, &k, sizeof(k1));
+    return gen2_res(test_gk1(cudaBlockSize, k1, vec, ref), "gk_K1");
+}
+
+gs2_formatData gs2_getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, const UIN th,
+                                    const char *mode, const gs2_matCSR m, const FPT *vec,
+                                    gs2_matAXT *a)
+{
+    const bool noc = mode && !strcmp(mode, "NOC"), com = mode && !strcmp(mode, "COM");
+    if (!noc && !com) {
+        gs::fail(GS_ERR_INVALID, "mode must be \"NOC\" or \"COM\"");
+        printf("getFormatDataAXT: mode must be \"NOC\" or \"COM\"\n");
+        return gen2_error_fd();
+    }
+    memset(a, 0, sizeof(*a));
+    a->nrows = m.nrows;
+    a->nnz = m.nnz;
+    snprintf(a->mode, sizeof(a->mode), "%s", mode);
+    a->tileHW = thw;
+    a->tileH = th;
+    for (UIN i = 0; i < 10; i++)
+        if ((th >> i) == 1) a->logTH = i;
+    if (com)
+        for (UIN i = 1; i < 10; i++)
+            if ((bs >> i) == 1) {
+                a->log = i;
+                break;
+            }
+    a->lenCON = m.nrows;
+    double ct = 0.0;
+    if (noc || th == 1) {
+        str_matAXT t;
+        memset(&t, 0, sizeof(t));
+        const str_formatData fd =
+            getFormatDataAXT(ompNT, bs, thw, th, noc ? "UNC" : "COM", gen1_view(m), vec, &t);
+        if (!strcmp(fd.name, "error")) return gen2_error_fd();
+        ct = fd.ct;
+        a->tileN = t.tileN;
+        a->lenAX = t.lenAX;
+        a->lenSEC = t.lenSEC;
+        a->ax = t.ax;
+        a->sec = t.sec;
+        a->con = t.con;  // the same values for rows < n (NOC); rebuilt below for COM
+    } else {
+        // COM with tileH > 1: lengths only, no array filled (gpuSpmv_header.h:1289-1301)
+        uint64_t cols = 0;
+        for (UIN r = 0; r < m.nrows; r++) cols += (m.row[r + 1] - m.row[r] + th - 1) / th;
+        a->tileN = (UIN)((cols + thw - 1) / thw);
+        a->lenAX = a->tileN * 2 * thw * th;
+        a->lenSEC = a->tileN * thw * th;
+        a->ax = (FPT *)calloc(a->lenAX ? a->lenAX : 1, sizeof(FPT));
+        a->sec = (UIN *)calloc(a->lenSEC ? a->lenSEC : 1, sizeof(UIN));
+    }
+    if (com) {
+        free(a->con);
+        a->con = (UIN *)calloc((size_t)m.nrows + 1, sizeof(UIN));
+        DevBuf row, sec, con;
+        const bool fill_sec = th == 1;
+        gs_status st = h2d(row, m.row, (size_t)m.nrows + 1);
+        if (!st && fill_sec) st = sec.alloc_zero((size_t)a->lenSEC * 4, 0);
+        if (!st) st = con.alloc(((size_t)m.nrows + 1) * 4);
+        if (st) return gen2_error_fd();
+        if (m.nrows)
+            k_gen2_com<<<(m.nrows + 255) / 256, 256>>>(m.nrows, row.as<UIN>(), thw, th, a->log,
+                                                       fill_sec ? sec.as<UIN>() : nullptr,
+                                                       con.as<UIN>());
+        if (cudaDeviceSynchronize() != cudaSuccess) return gen2_error_fd();
+        if (fill_sec && a->lenSEC)
+            cudaMemcpy(a->sec, sec.p, (size_t)a->lenSEC * 4, cudaMemcpyDeviceToHost);
+        if (m.nrows) cudaMemcpy(a->con, con.p, (size_t)m.nrows * 4, cudaMemcpyDeviceToHost);
+    }
+    char name[32];
+    snprintf(name, sizeof(name), "AXT_%s_H%u_HW%u", mode, th, thw);
+    return gen2_fd(name, (double)a->lenAX * sizeof(FPT) + (double)a->lenSEC * sizeof(UIN),
+                   (double)a->nnz / (double)(a->lenAX >> 1), ct);
+}
+
+gs2_res gs2_test_gk_AXT_NOC_H1(const UIN cudaBlockSize, const gs2_matAXT a, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    char name[24];
+    snprintf(name, sizeof(name), "gk_AXT_NOC_H1_HW%u", a.tileHW);
+    std::vector<UIN> ext;
+    return gen2_res(test_unc1("gk_AXT_NOC_H1", 0, gen1_axt(a, "UNC", ext), ref), name);
+}
+
+gs2_res gs2_test_gk_AXT_NOC(const UIN cudaBlockSize, const gs2_matAXT a, const FPT *ref)
+{
+    char name[24];
+    snprintf(name, sizeof(name), "gk_AXT_NOC_H%u_HW%u", a.tileH, a.tileHW);
+    std::vector<UIN> ext;
+    return gen2_res(test_gaxtuh(0, cudaBlockSize, gen1_axt(a, "UNC", ext), ref), name);
+}
+
+gs2_res gs2_test_gk_AXT_COM_H1(const UIN cudaBlockSize, const gs2_matAXT a, const FPT *ref)
+{
+    (void)cudaBlockSize;
+    char name[24];
+    snprintf(name, sizeof(name), "gk_AXT_COM_H1_HW%u", a.tileHW);
+    if (strcmp(a.mode, "COM") != 0 || a.tileH != 1) {
+        gs2_res r;
+        memset(&r, 0, sizeof(r));
+        strcpy(r.name, "error");
+        printf("%s: matrix is not a COM tileH=1 AXT layout\n", name);
+        return r;
+    }
+    DevBuf con, rpos;
+    str_res r1;
+    if (h2d(con, a.con, a.nrows) || rpos.alloc(((size_t)a.nrows + 1) * 4)) {
+        r1 = error_res(name, gs_last_error());
+    } else {
+        k_gen2_com_rpos<<<(a.nrows + 256) / 256, 256>>>(a.nrows, a.nnz, con.as<UIN>(), a.tileHW,
+                                                        rpos.as<UIN>());
+        r1 = run_baked(name, a.nrows, a.nnz, a.ax, a.lenAX, rpos, false, a.tileHW, 1, a.tileHW,
+                       0, ref);
+    }
+    return gen2_res(r1, name);
 }
 
 }  // extern "C"

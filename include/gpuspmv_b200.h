@@ -34,8 +34,23 @@ extern "C" {
  * 1. Drop-in layer (reference: cudaSpmv.cu)
  * ==================================================================================== */
 
+#ifndef GS_UIN_DEFINED
+#define GS_UIN_DEFINED
 typedef unsigned int UIN; /* cudaSpmv.cu:78-80 */
 typedef double FPT;       /* cudaSpmv.cu:64-74 with FP_TYPE == FP_DOUBLE */
+#endif
+
+/* GS_API_GEN2 selects the reference's second API generation (gpuSpmv_header.h) for the
+ * drop-in names instead of the first (cudaSpmv.cu); see gpuspmv_b200_gen2.h. */
+#ifdef GS_API_GEN2
+#ifdef __cplusplus
+}
+#endif
+#include "gpuspmv_b200_gen2.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+#else
 
 /* cudaSpmv.cu:261 */
 typedef struct {
@@ -185,6 +200,7 @@ str_res test_gaxtuh1hw04w(const UIN wpw, const UIN cbs, const str_matAXT matAXT,
 str_res test_gaxtuh(const UIN tpw, const UIN cbs, const str_matAXT matAXT, const FPT *ref);
 str_res test_gaxtch1(const UIN cudaBlockSize, const str_matAXT matAXT, const FPT *ref);
 str_res test_gaxtch(const UIN cudaBlockSize, const str_matAXT matAXT, const FPT *ref);
+#endif /* GS_API_GEN2 */
 
 /* ======================================================================================
  * 2. Native layer

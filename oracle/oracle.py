@@ -27,6 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "liboracle_port.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_oracle.so")
 REF_SPMV_SO = os.path.join(HERE, "_ref", "libref_spmv.so")
+REF_GEN2_SO = os.path.join(HERE, "_ref", "libref_gen2.so")
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -372,4 +373,101 @@ class Ref:
         out["name"] = name.value.decode()
         self.lib.ref_axt_copy(h, out["ax"], out["sec"], out["con"])
         self.lib.ref_axt_free(h)
+        return out
+
+
+class Ref2:
+    """The reference's second API generation (gpuSpmv_header.h), compiled unchanged
+    (oracle/_ref/libref_gen2.so)."""
+
+    _lib = None
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_GEN2_SO)
+
+    def __init__(self):
+        with _lock:
+            if Ref2._lib is None:
+                if not os.path.exists(REF_GEN2_SO):
+                    raise FileNotFoundError(f"{REF_GEN2_SO} missing: `make -C oracle ref`")
+                lib = C.CDLL(REF_GEN2_SO)
+                u32 = C.c_uint32
+                sig = {
+                    "ref2_stats": (None, [C.c_char_p, u32, u32, _f64p, _u32p, _u32p, _u32p, _f64p]),
+                    "ref2_cf_csr": (None, [u32, u32, _f64p, _u32p, _u32p, _f64p, _f64p]),
+                    "ref2_fd": (None, [C.c_char_p, _f64p]),
+                    "ref2_axc": (None, [u32, u32, u32, _f64p, _u32p, _u32p, _f64p, _u32p]),
+                    "ref2_axc_copy": (None, [_f64p, _u32p]),
+                    "ref2_k1": (None, [u32, u32, u32, _f64p, _u32p, _u32p, _f64p, _u32p]),
+                    "ref2_k1_copy": (None, [_u32p, _u32p, _u32p, _f64p, _u32p]),
+                    "ref2_axt": (None, [u32, u32, u32, u32, C.c_char_p, u32, u32, _f64p,
+                                        _u32p, _u32p, _f64p, _u32p]),
+                    "ref2_axt_copy": (None, [_f64p, _u32p, _u32p]),
+                }
+                for name, (res, args) in sig.items():
+                    f = getattr(lib, name)
+                    f.restype = res
+                    f.argtypes = args
+                Ref2._lib = lib
+        self.lib = Ref2._lib
+
+    def _fd(self):
+        name = C.create_string_buffer(18)
+        mb = np.zeros(2)
+        self.lib.ref2_fd(name, mb)
+        return {"name": name.value.decode(), "mfp": mb[0], "beta": mb[1]}
+
+    def stats(self, path, row, col, val):
+        row, col, val = _u32(row), _u32(col), _f64(val)
+        n = len(row) - 1
+        rl = np.zeros(max(n, 1), np.uint32)
+        out = np.zeros(5)
+        self.lib.ref2_stats(path.encode(), n, len(col), val, col, row, rl, out)
+        return rl[:n], dict(zip(("rmin", "rave", "rmax", "rsd", "bw"), out))
+
+    def cf_csr(self, row, col, val, x):
+        row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)
+        n = len(row) - 1
+        y = np.empty(n)
+        self.lib.ref2_cf_csr(n, len(col), val, col, row, x, y)
+        return y
+
+    def axc(self, row, col, val, x, threads=1):
+        row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)
+        n = len(row) - 1
+        dims = np.zeros(2, np.uint32)
+        self.lib.ref2_axc(threads, n, len(col), val, col, row, x, dims)
+        ax = np.zeros(int(dims[0]))
+        brp = np.zeros(int(dims[1]), np.uint32)
+        self.lib.ref2_axc_copy(ax, brp)
+        return {"lenAX": int(dims[0]), "lenBRP": int(dims[1]), "ax": ax, "brp": brp,
+                "fd": self._fd()}
+
+    def k1(self, row, col, val, x, cbs=32):
+        row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)
+        n = len(row) - 1
+        dims = np.zeros(2, np.uint32)
+        self.lib.ref2_k1(cbs, n, len(col), val, col, row, x, dims)
+        nc, lv = int(dims[0]), int(dims[1])
+        out = {"chunkNum": nc, "lenVC": lv, "permi": np.zeros(nc * 32, np.uint32),
+               "nmc": np.zeros(nc, np.uint32), "chp": np.zeros(nc, np.uint32),
+               "val": np.zeros(lv), "col": np.zeros(lv, np.uint32)}
+        self.lib.ref2_k1_copy(out["permi"], out["nmc"], out["chp"], out["val"], out["col"])
+        out["fd"] = self._fd()
+        return out
+
+    def axt(self, row, col, val, x, thw, th, mode, bs=256, threads=1):
+        row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)
+        n = len(row) - 1
+        dims = np.zeros(6, np.uint32)
+        self.lib.ref2_axt(threads, bs, thw, th, mode.encode(), n, len(col), val, col, row, x,
+                          dims)
+        keys = ("tileN", "lenAX", "lenSEC", "lenCON", "logTH", "log")
+        out = {k: int(v) for k, v in zip(keys, dims)}
+        out["ax"] = np.zeros(out["lenAX"])
+        out["sec"] = np.zeros(out["lenSEC"], np.uint32)
+        out["con"] = np.zeros(out["lenCON"], np.uint32)
+        self.lib.ref2_axt_copy(out["ax"], out["sec"], out["con"])
+        out["fd"] = self._fd()
         return out
