@@ -48,6 +48,8 @@ WORKLOADS = {
                            "x U[-1,1]", seed=0, xseed=0),
     "stencil27": dict(desc="3D 27-point stencil 160^3 (4096000 rows, 109215352 nnz), FP64, "
                            "x N(0,1)", seed=2, xseed=2),
+    "stencil27-small": dict(desc="3D 27-point stencil 100^3 (1000000 rows, 26463592 nnz, "
+                                 "profiling case), x N(0,1)", seed=2, xseed=2),
 }
 
 VARIANTS = {
@@ -124,8 +126,9 @@ def make_matrix(workload: str, rank: int):
     elif workload == "laplacian":
         row, col, val = matgen.laplacian2d(512)
         x = matgen.vector(len(row) - 1, "uniform", -1.0, 1.0, seed=w["xseed"] + rank)
-    elif workload == "stencil27":
-        row, col, val = matgen.stencil27(160, seed=w["seed"] + rank)
+    elif workload in ("stencil27", "stencil27-small"):
+        g = 160 if workload == "stencil27" else 100
+        row, col, val = matgen.stencil27(g, seed=w["seed"] + rank)
         x = matgen.vector(len(row) - 1, "normal", seed=w["xseed"] + rank)
     else:
         raise KeyError(workload)
@@ -276,8 +279,10 @@ def time_mixed(steps: int):
     out = {"workload": "27-point stencil 160^3 (4096000 rows, %d nnz), x N(0,1), seed 2" % nnz}
     dx64 = torch.from_numpy(x).cuda()
     for name, kw, acc in (("k1-f64", {}, False), ("k1-f32", dict(vtype="f32"), False),
+                          ("k1-f32-u16", dict(vtype="f32", itype="u16"), False),
                           ("k1-f32-acc64", dict(vtype="f32"), True),
-                          ("k1-bf16", dict(vtype="bf16"), False)):
+                          ("k1-bf16", dict(vtype="bf16"), False),
+                          ("k1-bf16-u16", dict(vtype="bf16", itype="u16"), False)):
         A = E.Matrix(row, col, val, ncols=n, fmt="K1", **kw)
         dx = dx64 if not kw else dx64.float()
         y = torch.empty(n, dtype=torch.float64 if (not kw or acc) else torch.float32,
@@ -287,7 +292,11 @@ def time_mixed(steps: int):
         out[name] = {"us": round(us, 2), "gflops": round(2.0 * nnz / us / 1e3, 1),
                      "error_vs_fp64": err}
         A.close()
-    out["speedup_f32_vs_f64"] = round(out["k1-f64"]["us"] / out["k1-f32"]["us"], 3)
+    ok = [k for k, v in out.items() if isinstance(v, dict) and k != "k1-f64"
+          and v["error_vs_fp64"] <= 1e-6]
+    best = min(ok, key=lambda k: out[k]["us"])
+    out["best_within_1e-6"] = best
+    out["speedup_vs_f64"] = round(out["k1-f64"]["us"] / out[best]["us"], 3)
     return out
 
 
@@ -435,6 +444,7 @@ def time_formats(row, col, val, x, steps: int):
     old = L.lib().gs_get_num_ite()
     L.lib().gs_set_num_ite(max(20, steps // 2))
     try:
+        L.lib().test_gcucsr(h.s, R.f64p(x), R.f64p(ref))  # warm-up: the library's first call
         r = L.lib().test_gcucsr(h.s, R.f64p(x), R.f64p(ref))
         out["cusparse-csr"] = round(r.et * 1e6, 2) if r.name == b"gcucsr" else None
     finally:

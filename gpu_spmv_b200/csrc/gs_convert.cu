@@ -114,32 +114,34 @@ __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
 template <class VIN, class VOUT>
 __global__ void k_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col,
                           const VIN *val, const uint32_t *permi, const uint32_t *chp,
-                          VOUT *oval, uint32_t *ocol)
+                          const uint32_t *nmc, bool blocked, VOUT *oval, uint32_t *ocol)
 {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
     const uint32_t r = permi[g], b = row[r], len = row[r + 1] - b;
-    const uint32_t base = chp[g / 32] + (g % 32);
+    const uint32_t c = g / 32, cb = chp[c], m = nmc[c];
     for (uint32_t e = 0; e < len; e++) {
-        oval[base + 32u * e] = cvt<VIN, VOUT>(val[b + e]);
-        ocol[base + 32u * e] = col[b + e];
+        const uint32_t pos = k1_slot(cb, m, e, g % 32, blocked);
+        oval[pos] = cvt<VIN, VOUT>(val[b + e]);
+        ocol[pos] = col[b + e];
     }
 }
 
 template <class VIN>
 void launch_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col, const VIN *val,
-                    const uint32_t *permi, const uint32_t *chp, gs_dtype vout, void *oval,
-                    uint32_t *ocol, cudaStream_t s)
+                    const uint32_t *permi, const uint32_t *chp, const uint32_t *nmc,
+                    bool blocked, gs_dtype vout, void *oval, uint32_t *ocol, cudaStream_t s)
 {
     const unsigned b = (n + 255) / 256;
     if (vout == GS_F64)
-        k_fill_k1<VIN, double><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+        k_fill_k1<VIN, double><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc, blocked,
                                                  static_cast<double *>(oval), ocol);
     else if (vout == GS_F32)
-        k_fill_k1<VIN, float><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+        k_fill_k1<VIN, float><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc, blocked,
                                                 static_cast<float *>(oval), ocol);
     else
-        k_fill_k1<VIN, __nv_bfloat16><<<b, 256, 0, s>>>(n, row, col, val, permi, chp,
+        k_fill_k1<VIN, __nv_bfloat16><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc,
+                                                        blocked,
                                                         static_cast<__nv_bfloat16 *>(oval),
                                                         ocol);
 }
@@ -316,14 +318,15 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
         DevBuf col32;  // 32-bit columns before the 16-bit steps are taken
         if (u16) GS_TRY(col32.alloc_zero((size_t)A->lenVC * 4, s));
         uint32_t *ocol = u16 ? col32.as<uint32_t>() : A->col.as<uint32_t>();
+        // 16-bit steps: lane-blocked slot order (k1_slot); otherwise the reference's
         if (val_type == GS_F64)
             launch_fill_k1<double>(n, d_row, d_col, static_cast<const double *>(d_val),
-                                   A->permi.as<uint32_t>(), A->chp.as<uint32_t>(), p.vtype,
-                                   A->val.p, ocol, s);
+                                   A->permi.as<uint32_t>(), A->chp.as<uint32_t>(),
+                                   A->nmc.as<uint32_t>(), u16, p.vtype, A->val.p, ocol, s);
         else
             launch_fill_k1<float>(n, d_row, d_col, static_cast<const float *>(d_val),
-                                  A->permi.as<uint32_t>(), A->chp.as<uint32_t>(), p.vtype,
-                                  A->val.p, ocol, s);
+                                  A->permi.as<uint32_t>(), A->chp.as<uint32_t>(),
+                                  A->nmc.as<uint32_t>(), u16, p.vtype, A->val.p, ocol, s);
         GS_CHECK_LAUNCH();
         GS_TRY(build_k1_plan(A->nmc.as<uint32_t>(), chunkNum, A->k1unit_chunk, A->k1unit_base,
                              A->k1partial, A->k1count, &A->k1units, s));
@@ -331,6 +334,7 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
             K1Args a{};
             a.nrows = n;
             a.chunkNum = chunkNum;
+            a.nmc = A->nmc.as<uint32_t>();
             a.chp = A->chp.as<uint32_t>();
             a.klen = A->k1len.as<uint32_t>();
             a.unit_chunk = A->k1unit_chunk.as<uint32_t>();

@@ -194,6 +194,19 @@ RowsArgs rows_args(const RowsPlan &P);
 gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
                       uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s);
 
+// Slot of step j of lane `lane` in the K1 chunk that starts at slot cbase and has nmc
+// steps.  The reference's order is cbase + 32 j + lane (a warp's loads of one step are
+// consecutive).  The 16-bit-step layouts use a lane-blocked order instead: steps below
+// 8 floor(nmc / 8) in groups of 8, each lane's 8 slots of a group consecutive
+// (cbase + 256 (j / 8) + 8 lane + j % 8), so that one 16-byte load brings a lane 8 steps;
+// the remaining steps keep the reference's order after them.
+__host__ __device__ __forceinline__ uint32_t k1_slot(uint32_t cbase, uint32_t nmc, uint32_t j,
+                                                     uint32_t lane, bool blocked)
+{
+    if (blocked && j < (nmc & ~7u)) return cbase + (j >> 3) * 256u + lane * 8u + (j & 7u);
+    return cbase + 32u * j + lane;
+}
+
 // K1 SpMV (see gs_spmv_k1.cu).
 struct K1Args {
     uint32_t nrows, chunkNum;

@@ -48,8 +48,40 @@ __device__ __forceinline__ AT k1_fma(AT acc, VT v, XT x)
     }
 }
 
+// 8 consecutive values of a lane-blocked group as floats (16- or 32-byte streaming loads)
+__device__ __forceinline__ void ld8_vals(const float *p, float (&v)[8])
+{
+    const float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
+    const float4 b = __ldcs(reinterpret_cast<const float4 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void ld8_vals(const __nv_bfloat16 *p, float (&v)[8])
+{
+    const uint4 w = __ldcs(reinterpret_cast<const uint4 *>(p));
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&ws[i]));
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+template <class T> __device__ __forceinline__ void ld8_vals(const T *, float (&)[8]) {}
+// 8 consecutive 16-bit column steps (one 16-byte streaming load)
+__device__ __forceinline__ void ld8_steps(const uint16_t *p, uint32_t (&c)[8])
+{
+    const uint4 w = __ldcs(reinterpret_cast<const uint4 *>(p));
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        c[2 * i] = ws[i] & 0xffffu;
+        c[2 * i + 1] = ws[i] >> 16;
+    }
+}
+
 template <class VT, class IT, class AT, class YT>
-__global__ void __launch_bounds__(256) k_k1(const K1Args a)
+__global__ void __launch_bounds__(256, std::is_same<VT, double>::value ? 8 : 6) k_k1(const K1Args a)
 {
     using XT = typename std::conditional<std::is_same<VT, double>::value, double, float>::type;
     constexpr bool kDelta = std::is_same<IT, uint16_t>::value;
@@ -76,8 +108,30 @@ __global__ void __launch_bounds__(256) k_k1(const K1Args a)
         if constexpr (kDelta) run = j0 < j1 ? __ldg(a.ck + (size_t)u * 32 + lane) : 0u;
         AT acc = AT(0);
         uint32_t j = j0;
+        if constexpr (kDelta) {
+            // lane-blocked groups of 8 steps: one 16-byte load of 8 column steps and one
+            // or two of 8 values (k1_slot); steps past this lane's row are padding
+            const uint32_t jg = min(j1, nmc & ~7u), cb = __ldg(a.chp + c);
+            for (; j < jg; j += 8) {
+                const uint32_t gp = cb + (j >> 3) * 256u + (uint32_t)lane * 8u;
+                float v[8];
+                uint32_t cc[8];
+                ld8_vals(val + gp, v);
+                ld8_steps(reinterpret_cast<const uint16_t *>(col) + gp, cc);
+                XT xv[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    run += cc[k];
+                    xv[k] = j + k < j1 ? __ldg(x + run) : XT(0);
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (j + k < j1) acc = k1_fma<float, XT, AT>(acc, v[k], xv[k]);
+            }
+        }
         // 8 slots in flight per lane: loads first, then gathers, then the ordered sum
-        for (; j + 8 <= j1; j += 8) {
+        // (16-bit steps: fewer than 8 steps remain after the groups)
+        for (; !kDelta && j + 8 <= j1; j += 8) {
             VT v[8];
             XT xv[8];
             uint32_t cc[8];
@@ -149,15 +203,16 @@ __global__ void __launch_bounds__(256) k_k1_deltas(const K1Args a, const uint32_
         const uint32_t len = g < a.nrows ? a.klen[g] : 0u;
         const uint32_t j0 = piece * kK1Split;
         const uint32_t j1 = min(len, j0 + kK1Split);
-        const uint32_t base = a.chp[c] + (uint32_t)lane;
-        uint32_t prev = j0 < j1 ? col32[base + 32u * j0] : 0u;
+        const uint32_t cb = a.chp[c], m = a.nmc[c];
+        uint32_t prev = j0 < j1 ? col32[k1_slot(cb, m, j0, lane, true)] : 0u;
         ck[(size_t)u * 32 + lane] = prev;
         bool bad = false;
         for (uint32_t j = j0; j < j1; j++) {
-            const uint32_t cj = col32[base + 32u * j];
+            const uint32_t pos = k1_slot(cb, m, j, lane, true);
+            const uint32_t cj = col32[pos];
             const uint32_t d = cj - prev;  // wraps when the row's columns decrease
             bad |= d > 0xffffu;
-            col16[base + 32u * j] = (uint16_t)d;
+            col16[pos] = (uint16_t)d;
             prev = cj;
         }
         if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, 1u);

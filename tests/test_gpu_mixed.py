@@ -38,6 +38,20 @@ def _bf16_round(a: np.ndarray) -> np.ndarray:
     return np.where(a == 0, a, np.rint(a / ulp) * ulp)
 
 
+def _k1_blocked(vals, nmc, chp):
+    """Reference-order K1 slots -> the lane-blocked order of the 16-bit-step layouts:
+    step j < 8 floor(nmc / 8) of lane l goes to chp + 256 (j / 8) + 8 l + j % 8."""
+    out = vals.copy()
+    for m, cb in zip(nmc.astype(np.int64), chp.astype(np.int64)):
+        j8 = m & ~7
+        if not j8:
+            continue
+        j = np.arange(j8)[:, None]
+        lane = np.arange(32)[None, :]
+        out[cb + (j // 8) * 256 + lane * 8 + j % 8] = vals[cb + 32 * j + lane]
+    return out
+
+
 @pytest.mark.parametrize("name", ["mixed", "row0_empty", "dense_row", "powerlaw_small",
                                   "laplacian"])
 @pytest.mark.parametrize("layout", LAYOUTS, ids=[_ids(p) for p in LAYOUTS])
@@ -64,7 +78,11 @@ def test_reduced_precision_bound(port, name, layout, vtype, itype, acc):
     err = np.abs(y - exact)
     assert np.all(err <= tol * mag), float(np.max(err / np.maximum(tol * mag, 1e-300)))
     # the stored values are the rounded FP64 values, in the same slots as FP64 storage
-    ref = E.Matrix(row, col, val, ncols=ncols, fmt=fmt, **kw).layout()["val"]
+    # (16-bit-step K1: the same slots in the lane-blocked order)
+    lay64 = E.Matrix(row, col, val, ncols=ncols, fmt=fmt, **kw).layout()
+    ref = lay64["val"]
+    if fmt == "K1" and itype == "u16":
+        ref = _k1_blocked(ref, lay64["nmc"], lay64["chp"])
     got = A.layout()["val"]
     if vtype == "f32":
         assert np.array_equal(got, ref.astype(np.float32))
