@@ -355,7 +355,7 @@ def time_adjoint(steps: int):
                     "slots = values kept in the adjoint layout's order"}
 
 
-def time_batched(steps: int):
+def time_batched(steps: int, count: int = 256):
     """256 banded matrices (rows log-uniform in [1000, 200000], half-bandwidth U[16, 256],
     U[5, 60] entries per row in the band, FP32 values N(0,1)), each with U[1, 32]
     right-hand sides N(0,1), seed 3: one persistent launch replayed from a CUDA graph, block
@@ -368,7 +368,7 @@ def time_batched(steps: int):
     from gpu_spmv_b200 import matgen
 
     rng = np.random.default_rng(3)
-    nm = 256
+    nm = count
     nrows = np.exp(rng.uniform(np.log(1000), np.log(200000), nm)).astype(np.int64)
     hbw = rng.integers(16, 257, nm)
     ks = [int(k) for k in rng.integers(1, 33, nm)]
@@ -394,8 +394,8 @@ def time_batched(steps: int):
     us_default = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
     B.set_blocking(kb_tuned)
     flops = B.flops
-    out = {"workload": "256 banded FP32 matrices, %d rows, %d nnz, 1-32 RHS (sum %d), seed 3"
-                       % (int(nrows.sum()), nnz_tot, sum(ks)),
+    out = {"workload": "%d banded FP32 matrices, %d rows, %d nnz, 1-32 RHS (sum %d), seed 3"
+                       % (nm, int(nrows.sum()), nnz_tot, sum(ks)),
            "us_per_run": round(us, 1), "gflops": round(flops / us / 1e3, 1),
            "us_per_run_untuned": round(us_default, 1),
            "work_items": B.nitems,
@@ -712,12 +712,25 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--only", choices=["mixed", "adjoint", "batched", "batched-small"],
+                    help="run one extension section alone and print its object")
     ap.add_argument("--format-steps", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.only:
+        # one section alone (profiling): its JSON object, `--steps` timed launches
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        fn = {"mixed": lambda: time_mixed(args.steps),
+              "adjoint": lambda: time_adjoint(args.steps),
+              "batched": lambda: time_batched(args.steps),
+              "batched-small": lambda: time_batched(args.steps, count=32)}[args.only]
+        print(json.dumps({args.only: fn()}))
+        return 0
     return run_ours(args)
 
 
