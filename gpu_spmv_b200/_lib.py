@@ -177,6 +177,8 @@ SIGNATURES = {
     "gs_algorithmic_bytes": (C.c_double, [UIN, UIN, UIN, UIN, UIN, UIN, UIN, UIN]),
     "gs_spmv": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, UIN, _vp]),
     "gs_spmv_host": (_st, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_int, UIN, _vp]),
+    "gs_spmv_host_stream": (_st, [_vp, _vp, C.c_size_t, C.c_int, _vp, C.c_size_t, C.c_int, UIN,
+                                  UIN, _vp]),
     "gs_csr_spmv_f64": (_st, [UIN, UIN, UIN, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gs_k1_spmv_f64_static": (_st, [UIN, UIN, UIN, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gs_spmm": (_st, [_vp, _vp, _vp, C.c_int, UIN, _vp]),

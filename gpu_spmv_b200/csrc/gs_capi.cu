@@ -179,6 +179,62 @@ gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dty
     return GS_OK;
 }
 
+gs_status gs_spmv_host_stream(const gs_matrix *Ac, const void *h_x, size_t x_stride,
+                              gs_dtype xtype, void *h_y, size_t y_stride, gs_dtype ytype,
+                              UIN count, UIN flags, gs_stream stream)
+{
+    if (!Ac || (count && (!h_x || !h_y))) return gs::fail(GS_ERR_INVALID, "NULL argument");
+    if (!count) return GS_OK;
+    gs_matrix *A = const_cast<gs_matrix *>(Ac);  // the pipeline is a cache of the handle
+    HostPipe &P = A->pipe;
+    const size_t xb = (size_t)A->ncols * gs::dtype_size(xtype);
+    const size_t yb = (size_t)A->nrows * gs::dtype_size(ytype);
+    if (!P.ready || P.x[0].bytes < xb || P.y[0].bytes < yb) {
+        if (!P.in) {
+            GS_CUDA(cudaStreamCreateWithFlags(&P.in, cudaStreamNonBlocking));
+            GS_CUDA(cudaStreamCreateWithFlags(&P.out, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; b++) {
+                GS_CUDA(cudaEventCreateWithFlags(&P.xready[b], cudaEventDisableTiming));
+                GS_CUDA(cudaEventCreateWithFlags(&P.kdone[b], cudaEventDisableTiming));
+                GS_CUDA(cudaEventCreateWithFlags(&P.ydone[b], cudaEventDisableTiming));
+            }
+        }
+        for (int b = 0; b < 2; b++) {
+            GS_TRY(P.x[b].alloc(xb));
+            GS_TRY(P.y[b].alloc(yb));
+        }
+        P.ready = true;
+    }
+    cudaStream_t s = gs::cs(stream);
+    const char *hx = static_cast<const char *>(h_x);
+    char *hy = static_cast<char *>(h_y);
+    const size_t xs = x_stride * gs::dtype_size(xtype), ys = y_stride * gs::dtype_size(ytype);
+    // the first uses of each buffer wait for nothing earlier on the compute stream
+    GS_CUDA(cudaEventRecord(P.kdone[0], s));
+    GS_CUDA(cudaEventRecord(P.kdone[1], s));
+    GS_CUDA(cudaEventRecord(P.ydone[0], s));
+    GS_CUDA(cudaEventRecord(P.ydone[1], s));
+    for (UIN k = 0; k < count; k++) {
+        const int b = (int)(k & 1u);
+        // in: x_k into buffer b once product k-2 (the last reader of b) is done
+        GS_CUDA(cudaStreamWaitEvent(P.in, P.kdone[b], 0));
+        GS_CUDA(cudaMemcpyAsync(P.x[b].p, hx + (size_t)k * xs, xb, cudaMemcpyHostToDevice, P.in));
+        GS_CUDA(cudaEventRecord(P.xready[b], P.in));
+        // compute: product k once x_k is in and y_{k-2} is out of buffer b
+        GS_CUDA(cudaStreamWaitEvent(s, P.xready[b], 0));
+        GS_CUDA(cudaStreamWaitEvent(s, P.ydone[b], 0));
+        GS_TRY(gs_spmv(A, P.x[b].p, xtype, P.y[b].p, ytype, flags, stream));
+        GS_CUDA(cudaEventRecord(P.kdone[b], s));
+        // out: y_k to the host
+        GS_CUDA(cudaStreamWaitEvent(P.out, P.kdone[b], 0));
+        GS_CUDA(cudaMemcpyAsync(hy + (size_t)k * ys, P.y[b].p, yb, cudaMemcpyDeviceToHost, P.out));
+        GS_CUDA(cudaEventRecord(P.ydone[b], P.out));
+    }
+    GS_CUDA(cudaStreamSynchronize(P.out));
+    GS_CUDA(cudaStreamSynchronize(s));
+    return GS_OK;
+}
+
 gs_status gs_matrix_device_status(const gs_matrix *A, UIN *word, int reset)
 {
     if (!A || !word) return gs::fail(GS_ERR_INVALID, "NULL argument");

@@ -128,8 +128,28 @@ struct RowsPlan {
 };
 }  // namespace gs
 
+// Streams, events and double buffers of the host-streaming product (gs_spmv_host_stream),
+// made on its first call.
+struct HostPipe {
+    cudaStream_t in = nullptr, out = nullptr;
+    cudaEvent_t xready[2] = {}, kdone[2] = {}, ydone[2] = {};
+    gs::DevBuf x[2], y[2];
+    bool ready = false;
+    ~HostPipe()
+    {
+        for (int b = 0; b < 2; b++) {
+            if (xready[b]) cudaEventDestroy(xready[b]);
+            if (kdone[b]) cudaEventDestroy(kdone[b]);
+            if (ydone[b]) cudaEventDestroy(ydone[b]);
+        }
+        if (in) cudaStreamDestroy(in);
+        if (out) cudaStreamDestroy(out);
+    }
+};
+
 // ------------------------------------------------------------------ the matrix handle
 struct gs_matrix {
+    HostPipe pipe;
     gs_convert_params p{};
     uint32_t nrows = 0, ncols = 0, nnz = 0;
     // reference-layout dimensions

@@ -326,6 +326,16 @@ gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y
 gs_status gs_spmv_host(const gs_matrix *A, const void *h_x, void *d_xbuf, gs_dtype xtype,
                        void *h_y, void *d_ybuf, gs_dtype ytype, UIN flags, gs_stream stream);
 
+/* `count` products y_k = A x_k streamed from host memory: x_k at h_x + k x_stride
+ * elements, y_k to h_y + k y_stride (strides may be 0: the same host vector every time).
+ * Each x_k is copied in and each y_k copied out; uploads, products and downloads of
+ * consecutive vectors overlap on three streams with two device buffers each (made on the
+ * first call and kept with the matrix).  Host buffers should be pinned for the copies to
+ * overlap.  Returns when every y_k is on the host. */
+gs_status gs_spmv_host_stream(const gs_matrix *A, const void *h_x, size_t x_stride,
+                              gs_dtype xtype, void *h_y, size_t y_stride, gs_dtype ytype,
+                              UIN count, UIN flags, gs_stream stream);
+
 /* Synchronous device -> host copy of `bytes` bytes (for bindings that read a matrix's
  * device arrays back without a CUDA runtime of their own). */
 gs_status gs_copy_to_host(void *h_dst, const void *d_src, size_t bytes);

@@ -160,3 +160,32 @@ def test_com_header_overflow_reported():
     A = E.Matrix(row, col, val, fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=1024)
     x = torch.arange(n, dtype=torch.float64, device="cuda")
     assert torch.equal(A.spmv(x), x)
+
+
+@pytest.mark.parametrize("fmt,vtype", [("K1", "f64"), ("CSR", "f64"), ("K1", "f32")])
+def test_host_stream_products(port, fmt, vtype):
+    """gs_spmv_host_stream: each of several host vectors copied in, multiplied and copied
+    out, overlapped across vectors; every y_k equals the device product of x_k."""
+    import ctypes as C
+
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(8)
+    row, col, val = case("powerlaw_small", rng)
+    n = len(row) - 1
+    A = E.Matrix(row, col, val, ncols=n, fmt=fmt, vtype=vtype)
+    dt = torch.float64 if vtype == "f64" else torch.float32
+    code = L.GS_F64 if vtype == "f64" else L.GS_F32
+    k = 7
+    X = torch.from_numpy(rng.uniform(-1, 1, (k, n))).to(dt).pin_memory()
+    Y = torch.empty(k, n, dtype=dt).pin_memory()
+    L.check(L.lib().gs_spmv_host_stream(A._h, X.data_ptr(), n, code, Y.data_ptr(), n, code, k,
+                                        0, E.stream_handle()), "stream")
+    for i in range(k):
+        assert torch.equal(Y[i], A.spmv(X[i].cuda()).cpu()), i
+    # stride 0: the same vector every time, the last y stays
+    L.check(L.lib().gs_spmv_host_stream(A._h, X.data_ptr(), 0, code, Y.data_ptr(), 0, code, 3,
+                                        0, E.stream_handle()), "stream")
+    assert torch.equal(Y[0], A.spmv(X[0].cuda()).cpu())
+    A.close()
