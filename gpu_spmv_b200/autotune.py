@@ -1,4 +1,5 @@
-"""Autotuner for batched multi-RHS products: picks each matrix's right-hand-side block width.
+"""Autotuners: the layout of a single matrix (choose_format), and each matrix's
+right-hand-side block width in a batched multi-RHS product (tune).
 
 A matrix with kpad right-hand sides runs as kpad/kb passes of kb columns.  Wide blocks
 gather each stored element's x row once for all columns; narrow ones re-read the value and
@@ -92,3 +93,87 @@ def tune(batch: E.Batch, reps: int = 5, cache_path: str | None = None) -> dict:
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
     return {"choices": choices, "timings": timings}
+
+
+# ----------------------------------------------------------------------------- formats
+# Candidate layouts for one matrix (the reference sweeps these by hand: its job scripts run
+# every format and tile parameter and compare the timings).
+FORMAT_CANDIDATES = {
+    "k1": dict(fmt="K1"),
+    "csr": dict(fmt="CSR"),
+    "axt-unc-th4": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
+    "axt-unc-th8": dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
+    "axt-unc-th1-hw4": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
+    "axt-com-th1": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32),
+}
+
+
+def matrix_key(row, vtype: str = "f64") -> str:
+    """Shape class of a CSR matrix: dtype, log2 rows, log2 nnz, row-length spread."""
+    import numpy as np
+
+    row = np.asarray(row, dtype=np.int64)
+    n = len(row) - 1
+    nnz = int(row[-1])
+    lens = np.diff(row)
+    cv = float(lens.std() / max(lens.mean(), 1e-9)) if n else 0.0
+    spread = 0 if cv < 0.25 else (1 if cv < 1.0 else 2)
+    return f"{vtype}/n2^{max(n, 1).bit_length()}/nnz2^{max(nnz, 1).bit_length()}/cv{spread}"
+
+
+def choose_format(row, col, val, ncols=None, vtype: str = "f64", candidates=None,
+                  reps: int = 20, cache_path: str | None = None, device="cuda"):
+    """Convert the matrix into each candidate layout, time its product (CUDA events,
+    median of `reps` after warm-up) and return (best Matrix, {name: µs}); the others are
+    released.  With a cache holding this matrix's key, only the cached choice is built."""
+    from . import _lib as L
+    from . import engine as E
+
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    key = matrix_key(row, vtype)
+    names = list(candidates or FORMAT_CANDIDATES)
+    if key in cache and cache[key] in FORMAT_CANDIDATES:
+        names = [cache[key]]
+    n = len(row) - 1
+    nc = ncols if ncols is not None else n
+    dt = torch.float64 if vtype == "f64" else torch.float32
+    x = torch.rand(nc, dtype=dt, device=device)
+    best, best_t, timings = None, float("inf"), {}
+    for name in names:
+        kw = dict(FORMAT_CANDIDATES[name])
+        try:
+            A = E.Matrix(row, col, val, ncols=nc, vtype=vtype, device=device, **kw)
+        except L.GSError as e:  # a layout this matrix or value type cannot take
+            if e.status != L.GS_ERR_UNSUPPORTED:
+                raise
+            continue
+        y = A.spmv(x)
+        for _ in range(3):
+            A.spmv(x, y)
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            A.spmv(x, y)
+            b.record()
+            ts.append((a, b))
+        torch.cuda.synchronize()
+        t = statistics.median(a.elapsed_time(b) for a, b in ts) * 1e3
+        timings[name] = t
+        if t < best_t:
+            if best is not None:
+                best.close()
+            best, best_t = A, t
+            best.autotuned_format = name
+        else:
+            A.close()
+    if best is None:
+        raise RuntimeError("no candidate layout accepted the matrix")
+    if cache_path and len(names) > 1:
+        cache[key] = best.autotuned_format
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return best, timings

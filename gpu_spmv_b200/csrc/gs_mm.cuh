@@ -108,10 +108,10 @@ __device__ __forceinline__ void store_row(T *__restrict__ Y, uint32_t r, uint32_
 
 // slots in flight per lane: at most 8, and at most 128 bytes of gathered rows (more
 // registers would cost occupancy, which the latency-bound gathers need more)
-template <class T, int K> constexpr int mm_batch()
+template <class T, int K, int BYTES = 128> constexpr int mm_batch()
 {
-    return (128 / (K * (int)sizeof(T))) < 1 ? 1
-           : ((128 / (K * (int)sizeof(T))) > 8 ? 8 : 128 / (K * (int)sizeof(T)));
+    return (BYTES / (K * (int)sizeof(T))) < 1 ? 1
+           : ((BYTES / (K * (int)sizeof(T))) > 8 ? 8 : BYTES / (K * (int)sizeof(T)));
 }
 
 struct MMArgs {
@@ -140,7 +140,8 @@ template <class T, int K, bool ADJ>
 __device__ __forceinline__ void mm_unit(const MMArgs &a, uint32_t u, uint32_t rb)
 {
     using A = Arith<T>;
-    constexpr int B = mm_batch<T, K>();
+    // the adjoint also holds X's row and the slot indices: half the gathered bytes in flight
+    constexpr int B = mm_batch<T, K, ADJ ? 64 : 128>();
     const uint32_t off = rb * K;
     const T *__restrict__ val = static_cast<const T *>(a.val);
     const T *__restrict__ xin = static_cast<const T *>(a.xin) + off;
