@@ -229,6 +229,46 @@ def cpu_reference_spmv(row, col, val, x, budget_s=15.0, threads=None):
     return 2.0 * nnz / dt / 1e9, f"{reps} full SpMVs of the workload ({nnz} nnz)", threads
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_details(row, col, val, x, block_rows: int = 1 << 18, reps: int = 5):
+    """Single-core figures on a bounded sample (the first `block_rows` rows): the
+    reference's ncsr on 1 thread and its serial cpuSpmvCSR (spmv_header.h), and the oracle's
+    restatement of the CPU AXT loop (UNC tileH=1, tileHW=16, column stream); median of
+    `reps` runs, GFLOP/s."""
+    from oracle.oracle import Port, Ref
+
+    R, P = Ref(), Port()
+    r1 = min(block_rows, len(row) - 1)
+    rr = np.ascontiguousarray(row[:r1 + 1])
+    cc, vv = col[:int(rr[-1])], val[:int(rr[-1])]
+    nnz = len(cc)
+
+    def med(fn):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return 2.0 * nnz / statistics.median(ts) / 1e9
+
+    a = P.axt(rr, cc, vv, 16, 1, "UNC")
+    out = {"sample": f"first {r1} rows ({nnz} nnz), median of {reps}",
+           "ncsr_1_thread": med(lambda: R.ncsr(rr, cc, vv, x, threads=1)),
+           "axt_unc_th1_hw16_restated_1_thread": med(lambda: P.axt_spmv(a, x))}
+    if R.lib_spmv is not None:
+        out["cpuSpmvCSR_serial"] = med(lambda: R.cpu_spmv_csr(rr, cc, vv, x))
+    return out
+
+
 def error_vs_fp64(row, col, val, x, y) -> float:
     """max_i |y_i - y64_i| / (|A||x|)_i of a reduced-precision product y against the FP64
     product (the engine's K1 FP64 path, itself within 1e-13 of the reference's CPU loop)."""
@@ -669,7 +709,8 @@ def run_ours(args):
         try:
             v, sample, threads = cpu_reference_spmv(row, col, val, x)
             cpu = {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference",
-                   "sample": sample + "; reference ncsr compiled unchanged (oracle/_ref)"}
+                   "sample": sample + "; reference ncsr compiled unchanged (oracle/_ref)",
+                   "cpu_model": cpu_model(), "one_core": cpu_details(row, col, val, x)}
         except Exception as e:  # the checker library is absent: report it
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
