@@ -316,7 +316,10 @@ gs_status gs_matrix_device_status(const gs_matrix *A, UIN *word, int reset);
 
 /* y = A x on the device.  x has ncols entries of xtype, y nrows entries of ytype.
  * F64 matrices take F64 x/y; F32/BF16 matrices take F32 x and F32 or F64 y.
- * Deterministic: every y entry is written once, with a fixed summation order. */
+ * Deterministic: every y entry is written once, with a fixed summation order.
+ * Products on one matrix (gs_spmv, gs_spmm, gs_spmm_adjoint, batches holding it) share its
+ * K1 split-chunk counters and status word: calls that could overlap in time (other
+ * streams, other threads) must be ordered by the caller. */
 gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y,
                   gs_dtype ytype, UIN flags, gs_stream stream);
 
