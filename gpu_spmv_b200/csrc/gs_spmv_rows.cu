@@ -545,8 +545,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 // lanes' first bits, and a row's lanes are joined by one segmented scan -- close to the
 // instruction count of a row-per-lane kernel while keeping the AXT tile layout's
 // coalesced loads.
+//
+// T32: tiled layouts with tileHW = 32 and tileH = V, where a window of 32 lanes x V positions
+// is exactly one tile and lane l owns its column l: element k of that column is slot
+// w * 32V + 32k + l, with no division by the runtime tile size.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
-          bool BAKED, bool PADDED, bool EMPTY>
+          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false>
 __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -602,11 +606,14 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                         p[k] = (PT)0;
                         if ((rb >> k) & 1u) {
                             uint32_t s = qb + k;
-                            if constexpr (TILED) {
+                            if constexpr (TILED && T32) {
+                                s = w * WS + 32u * (uint32_t)k + (uint32_t)lane;
+                            } else if constexpr (TILED) {
                                 const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
                                 s = t * ths + (uint32_t)k * a.thw + c;
                             }
-                            const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                            const uint32_t ai = T32 ? (s >> 5) * 64u + (s & 31u)
+                                                    : (s / a.axw) * 2u * a.axw + s % a.axw;
                             p[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
                         }
                     }
@@ -614,15 +621,22 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                     VT v[V];
                     IT c[V];
                     if constexpr (TILED) {
-                        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
-                        const uint32_t s0 = t * ths + cc;
+                        uint32_t s0, stride;
+                        if constexpr (T32) {
+                            s0 = w * WS + (uint32_t)lane;
+                            stride = 32u;
+                        } else {
+                            const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
+                            s0 = t * ths + cc;
+                            stride = a.thw;
+                        }
 #pragma unroll
                         for (int k = 0; k < V; k++) {
                             v[k] = (VT)0;
                             c[k] = 0;
                             if ((rb >> k) & 1u) {
-                                v[k] = ld_stream(val + s0 + (uint32_t)k * a.thw);
-                                c[k] = ld_stream(col + s0 + (uint32_t)k * a.thw);
+                                v[k] = ld_stream(val + s0 + (uint32_t)k * stride);
+                                c[k] = ld_stream(col + s0 + (uint32_t)k * stride);
                             }
                         }
                     } else {
@@ -997,8 +1011,16 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
     if (warps == 0) return GS_OK;
     uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
     const bool empty = a.n_empty != 0;
+    const bool t32 = TILED && a.thw == 32 && a.th == (uint32_t)V;
 #define GS_L(P, E)                                                                          \
-    k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E><<<blocks, 256, 0, s>>>(a)
+    do {                                                                                    \
+        if (t32)                                                                            \
+            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED>            \
+                <<<blocks, 256, 0, s>>>(a);                                                 \
+        else                                                                                \
+            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, false>            \
+                <<<blocks, 256, 0, s>>>(a);                                                 \
+    } while (0)
     if (padded) {
         if (empty) GS_L(true, true); else GS_L(true, false);
     } else {
