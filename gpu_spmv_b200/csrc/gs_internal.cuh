@@ -247,7 +247,8 @@ gs_status launch_k1(const K1Args &a, gs_dtype vtype, gs_itype itype, gs_dtype yt
 gs_status build_k1_deltas(const K1Args &a, const uint32_t *d_col32, uint16_t *d_col16,
                           uint32_t *d_ck, cudaStream_t s);
 // Build the K1 plan for chunk lengths nmc (device) into the given buffers.
-constexpr uint32_t kK1Split = 256;  // j-steps per K1 work unit
+constexpr uint32_t kK1Split = 128;  // j-steps per K1 work unit (a piece is a critical path of
+                                     // kK1Split/8 dependent gather rounds: 128 keeps it short)
 gs_status build_k1_plan(const uint32_t *d_nmc, uint32_t chunkNum, DevBuf &unit_chunk,
                         DevBuf &unit_base, DevBuf &partial, DevBuf &count, uint32_t *units,
                         cudaStream_t s);

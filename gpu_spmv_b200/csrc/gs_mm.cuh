@@ -1,6 +1,6 @@
 // gs_mm.cuh -- device code shared by the multi-RHS K1 kernels (gs_spmm.cu, gs_batch.cu):
 // arithmetic in the reference's order (separate multiply and add), 16/32-byte row access of
-// row-major [*][ld] operands, and the work of one K1 unit (one 256-step piece of a 32-row
+// row-major [*][ld] operands, and the work of one K1 unit (one kK1Split-step piece of a 32-row
 // chunk) for a block of K right-hand sides.
 #pragma once
 

@@ -4,7 +4,7 @@
 // k in {1, 2, 4, 8, 16, 32}) on the K1 layout.  Each lane owns one sorted row, as in the
 // single-RHS kernel (gs_spmv_k1.cu), and one gather of a column fetches all k values of
 // X's row at once (32 bytes for k = 8 in FP32), so the gather cost is paid once per
-// stored element for every right-hand side.  Long chunks are cut into the same 256-step
+// stored element for every right-hand side.  Long chunks are cut into the same kK1Split-step
 // pieces, whose partial sums meet in scratch memory in piece order.
 //
 // Adjoint, for a loss L(Y) with Ybar = dL/dY:
@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) k_k1_mm(const MMArgs a)
         mm_unit<T, K, ADJ>(a, u, 0);
 }
 
-// Atomic-mode adjoint on the forward layout, over the same 256-step work units: lane = row
+// Atomic-mode adjoint on the forward layout, over the same kK1Split-step work units: lane = row
 // r of A with Ybar[r] in registers; per stored element e: vbar_e = Ybar[r] . X[col_e] and
 // Xbar[col_e] += v_e Ybar[r] (atomic adds; Xbar zeroed first).
 struct AtomicArgs {

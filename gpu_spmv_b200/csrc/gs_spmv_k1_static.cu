@@ -1,6 +1,6 @@
 // gs_spmv_k1_static.cu -- K1 SpMV over caller-owned device arrays, allocating nothing.
 //
-// The K1 kernel of gs_spmv_k1.cu cuts chunks longer than kK1Split steps into pieces whose
+// The K1 kernel of gs_spmv_k1.cu cuts long chunks into pieces whose
 // partial sums meet in scratch memory (32 doubles per piece, one arrival counter per
 // chunk); gs_spmv keeps that scratch, and the piece plan, in the gs_matrix.  This variant
 // takes the arrays the reference's gk1 kernel takes (cudaSpmv.cu:851: val, col, nmc, chp,
@@ -39,6 +39,7 @@ namespace gs {
 
 namespace {
 
+constexpr uint32_t kStaticSplit = 256;     // steps per piece (the bound below assumes 256)
 constexpr uint32_t kStaticUnits = 32768;   // pieces of split chunks
 constexpr uint32_t kStaticChunks = 32768;  // split chunks
 constexpr size_t kPartialBytes = (size_t)kStaticUnits * 32 * sizeof(double);
@@ -64,7 +65,7 @@ struct K1StaticArgs {
     uint32_t *count, *unit_base, *hdr;
 };
 
-// One block: S = number of leading chunks longer than kK1Split (bisection on the sorted
+// One block: S = number of leading chunks longer than kStaticSplit (bisection on the sorted
 // nmc), unit_base[c] = first piece of chunk c < S, hdr = {S, pieces}; {0, 0} when the
 // prefix does not fit the scratch.
 __global__ void __launch_bounds__(1024) k_k1s_prefix(const K1StaticArgs a)
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(1024) k_k1s_prefix(const K1StaticArgs a)
         uint32_t lo = 0, hi = a.chunkNum;
         while (lo < hi) {
             const uint32_t mid = lo + (hi - lo) / 2;
-            if (__ldg(a.nmc + mid) > kK1Split) lo = mid + 1;
+            if (__ldg(a.nmc + mid) > kStaticSplit) lo = mid + 1;
             else hi = mid;
         }
         s_split = lo <= kStaticChunks ? lo : 0u;
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(1024) k_k1s_prefix(const K1StaticArgs a)
         const uint32_t c = b + t;
         uint32_t p = 0;
         if (c < S) {
-            p = (__ldg(a.nmc + c) + kK1Split - 1) / kK1Split;
+            p = (__ldg(a.nmc + c) + kStaticSplit - 1) / kStaticSplit;
             p = max(1u, min(p, kStaticUnits + 1));  // bounded: the sum cannot wrap
         }
         uint32_t v = p;
@@ -154,8 +155,8 @@ __global__ void __launch_bounds__(256) k_k1s(const K1StaticArgs a)
         const uint32_t g = 32u * c + (uint32_t)lane;
         const bool valid = g < a.nrows;
         const uint32_t len = valid ? __ldg(a.nmc + c) : 0u;
-        const uint32_t j0 = piece * kK1Split;
-        const uint32_t j1 = np == 1 ? len : min(len, j0 + kK1Split);
+        const uint32_t j0 = piece * kStaticSplit;
+        const uint32_t j1 = np == 1 ? len : min(len, j0 + kStaticSplit);
         const uint32_t base = __ldg(a.chp + c) + (uint32_t)lane;
         double acc = 0.0;
         uint32_t j = j0;
