@@ -172,6 +172,8 @@ SIGNATURES = {
     "gs_get_num_ite": (UIN, []),
     "gs_matrix_create": (_st, [C.POINTER(_vp), C.POINTER(ConvertParams), UIN, UIN, UIN, _vp,
                                _vp, _vp, C.c_int, _vp]),
+    "gs_matrix_create_host": (_st, [C.POINTER(_vp), C.POINTER(ConvertParams), UIN, UIN, UIN,
+                                    _vp, _vp, _vp, C.c_int, _vp]),
     "gs_matrix_destroy": (_st, [_vp]),
     "gs_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
     "gs_algorithmic_bytes": (C.c_double, [UIN, UIN, UIN, UIN, UIN, UIN, UIN, UIN]),

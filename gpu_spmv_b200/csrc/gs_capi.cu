@@ -63,6 +63,32 @@ gs_status gs_matrix_create(gs_matrix **out, const gs_convert_params *params, UIN
     return GS_OK;
 }
 
+gs_status gs_matrix_create_host(gs_matrix **out, const gs_convert_params *params, UIN nrows,
+                                UIN ncols, UIN nnz, const UIN *h_row, const UIN *h_col,
+                                const void *h_val, gs_dtype val_type, gs_stream stream)
+{
+    gs::clear_error();
+    if (!out || !params || !h_row || (nnz && (!h_col || !h_val)))
+        return gs::fail(GS_ERR_INVALID, "NULL argument");
+    if (val_type != GS_F64 && val_type != GS_F32)
+        return gs::fail(GS_ERR_UNSUPPORTED, "input CSR values must be FP64 or FP32");
+    *out = nullptr;
+    gs::DevBuf row, col, val;
+    const size_t vsz = gs::dtype_size(val_type);
+    GS_TRY(row.alloc(((size_t)nrows + 1) * 4));
+    GS_TRY(col.alloc((size_t)nnz * 4));
+    GS_TRY(val.alloc((size_t)nnz * vsz));
+    cudaStream_t s = gs::cs(stream);
+    GS_CUDA(cudaMemcpyAsync(row.p, h_row, ((size_t)nrows + 1) * 4, cudaMemcpyHostToDevice, s));
+    if (nnz) {
+        GS_CUDA(cudaMemcpyAsync(col.p, h_col, (size_t)nnz * 4, cudaMemcpyHostToDevice, s));
+        GS_CUDA(cudaMemcpyAsync(val.p, h_val, (size_t)nnz * vsz, cudaMemcpyHostToDevice, s));
+    }
+    // the conversion synchronises before returning, so the staging buffers may go
+    return gs_matrix_create(out, params, nrows, ncols, nnz, row.as<UIN>(), col.as<UIN>(),
+                            val.p, val_type, stream);
+}
+
 gs_status gs_matrix_destroy(gs_matrix *A)
 {
     if (A) {

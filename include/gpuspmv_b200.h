@@ -262,6 +262,11 @@ typedef struct gs_matrix gs_matrix;
 gs_status gs_matrix_create(gs_matrix **out, const gs_convert_params *params, UIN nrows,
                            UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
                            const void *d_val, gs_dtype val_type, gs_stream stream);
+/* The same from host CSR arrays (copied to the device on `stream`, then converted), for
+ * callers without a CUDA runtime of their own. */
+gs_status gs_matrix_create_host(gs_matrix **out, const gs_convert_params *params, UIN nrows,
+                                UIN ncols, UIN nnz, const UIN *h_row, const UIN *h_col,
+                                const void *h_val, gs_dtype val_type, gs_stream stream);
 gs_status gs_matrix_destroy(gs_matrix *A);
 
 /* Sizes and device arrays of a converted matrix (pointers stay owned by the matrix). */

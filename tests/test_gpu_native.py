@@ -189,3 +189,29 @@ def test_host_stream_products(port, fmt, vtype):
                                         0, E.stream_handle()), "stream")
     assert torch.equal(Y[0], A.spmv(X[0].cuda()).cpu())
     A.close()
+
+
+def test_create_from_host_arrays(port):
+    """gs_matrix_create_host: the same matrix as from device arrays, from host CSR arrays."""
+    import ctypes as C
+
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(12)
+    row, col, val = case("powerlaw_small", rng)
+    n = len(row) - 1
+    row = np.ascontiguousarray(row, np.uint32)
+    col = np.ascontiguousarray(col, np.uint32)
+    val = np.ascontiguousarray(val, np.float64)
+    p = L.ConvertParams(L.GS_FMT_AXT, 32, 4, 256, L.GS_AXT_UNC, 32, L.GS_F64, L.GS_IDX_U32, 0)
+    h = C.c_void_p()
+    L.check(L.lib().gs_matrix_create_host(C.byref(h), C.byref(p), n, n, len(col),
+                                          row.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                          L.GS_F64, None), "create_host")
+    x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    L.check(L.lib().gs_spmv(h, x.data_ptr(), L.GS_F64, y.data_ptr(), L.GS_F64, 0, None), "spmv")
+    A = E.Matrix(row, col, val, ncols=n, fmt="AXT", mode="UNC", tileH=4, tileHW=32)
+    assert torch.equal(y, A.spmv(x))
+    L.lib().gs_matrix_destroy(h)
