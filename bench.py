@@ -398,8 +398,9 @@ def time_adjoint(steps: int):
 def time_batched(steps: int, count: int = 256):
     """256 banded matrices (rows log-uniform in [1000, 200000], half-bandwidth U[16, 256],
     U[5, 60] entries per row in the band, FP32 values N(0,1)), each with U[1, 32]
-    right-hand sides N(0,1), seed 3: one persistent launch replayed from a CUDA graph, block
-    widths from the autotuner.  The plain FP64 form is the same work as single-RHS FP64 K1
+    right-hand sides N(0,1), seed 3: one persistent launch replayed from a CUDA graph (row
+    blocks with the X band in shared memory), block widths from the autotuner; beside it
+    the same batch on K1 units.  The plain FP64 form is the same work as single-RHS FP64 K1
     products, one per matrix and right-hand side (device time per product x k_i)."""
     import torch
 
@@ -433,12 +434,18 @@ def time_batched(steps: int, count: int = 256):
     B.set_blocking(B.kpad)
     us_default = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
     B.set_blocking(kb_tuned)
+    paths = B.paths
+    B.set_paths(["k1"] * nm)  # every matrix on K1 units (gathers through L1 / L2)
+    us_k1 = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
+    B.set_paths(["auto"] * nm)
     flops = B.flops
     out = {"workload": "%d banded FP32 matrices, %d rows, %d nnz, 1-32 RHS (sum %d), seed 3"
                        % (nm, int(nrows.sum()), nnz_tot, sum(ks)),
            "us_per_run": round(us, 1), "gflops": round(flops / us / 1e3, 1),
            "us_per_run_untuned": round(us_default, 1),
            "work_items": B.nitems,
+           "row_block_matrices": paths.count("band"),
+           "us_per_run_k1_units": round(us_k1, 1),
            "plain_fp64_us": round(plain_us, 1),
            "plain_fp64_gflops": round(flops / plain_us / 1e3, 1),
            "speedup_vs_plain_fp64": round(plain_us / us, 2),

@@ -29,6 +29,7 @@ GS_FLAG_NONE, GS_FLAG_ACC_F64, GS_FLAG_TMA, GS_FLAG_STRIPED = 0, 1, 2, 4
 GS_K1_STATIC_MAX_SLOTS = 134217728
 GS_ADJ_DETERMINISTIC, GS_ADJ_ATOMIC = 0, 1
 GS_VALUES_CSR, GS_VALUES_SLOTS = 0, 1
+GS_BATCH_AUTO, GS_BATCH_K1, GS_BATCH_BAND = 0, 1, 2
 
 
 # ------------------------------------------------------------------ drop-in structs
@@ -194,6 +195,9 @@ SIGNATURES = {
     "gs_batch_info": (_st, [_vp, C.POINTER(UIN), C.POINTER(UIN), C.POINTER(C.c_double)]),
     "gs_batch_set_operands": (_st, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "gs_batch_set_blocking": (_st, [_vp, C.POINTER(UIN), _vp]),
+    "gs_batch_set_paths": (_st, [_vp, C.POINTER(UIN), _vp]),
+    "gs_batch_paths": (_st, [_vp, C.POINTER(UIN)]),
+    "gs_batch_status": (_st, [_vp, C.POINTER(UIN), _vp]),
     "gs_batch_run": (_st, [_vp, _vp]),
     "gs_batch_run_graph": (_st, [_vp, _vp]),
     "gs_copy_to_host": (_st, [_vp, _vp, C.c_size_t]),

@@ -42,11 +42,14 @@
 
 #include <type_traits>
 
+#include "gs_bulk.cuh"
 #include "gs_internal.cuh"
 
 namespace gs {
 
 namespace {
+
+using namespace bulk;
 
 constexpr int kWarpsPerBlock = 8;
 constexpr int kTmaWarps = 4;   // warps per block of the TMA kernel
@@ -123,65 +126,6 @@ __device__ __forceinline__ uint32_t get_bits(const uint32_t *bm, uint32_t p, uin
     const uint32_t w = p >> 5, sh = p & 31;
     const uint64_t two = (uint64_t)__ldg(bm + w) | ((uint64_t)__ldg(bm + w + 1) << 32);
     return (uint32_t)(two >> sh) & (V >= 32 ? 0xffffffffu : ((1u << V) - 1u));
-}
-
-// ---- TMA bulk copy / mbarrier primitives (1-D bulk copies, no multicast)
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
-                                         uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait for an mbarrier phase: gives up after ~2 s of wall time.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > 2000000000ull) return false;
-    return true;
 }
 
 // ---------------------------------------------------------------------------------------

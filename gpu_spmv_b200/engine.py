@@ -361,6 +361,31 @@ class Batch:
                 "gs_batch_set_blocking")
         self.blocking = [int(b) for b in kb]
 
+    PATHS = {"auto": L.GS_BATCH_AUTO, "k1": L.GS_BATCH_K1, "band": L.GS_BATCH_BAND}
+
+    def set_paths(self, paths, stream=None):
+        """How each matrix runs: "k1" (warps over K1 units), "band" (thread blocks over row
+        blocks with the X band staged in shared memory) or "auto" (band where it fits)."""
+        n = len(self.mats)
+        arr = (L.UIN * max(1, n))(*[self.PATHS[p] for p in paths])
+        L.check(L.lib().gs_batch_set_paths(self._h, arr, stream_handle(stream)),
+                "gs_batch_set_paths")
+
+    @property
+    def paths(self):
+        """The path each matrix runs on: "k1" or "band"."""
+        n = len(self.mats)
+        arr = (L.UIN * max(1, n))()
+        L.check(L.lib().gs_batch_paths(self._h, arr), "gs_batch_paths")
+        return ["band" if arr[i] == L.GS_BATCH_BAND else "k1" for i in range(n)]
+
+    def status(self, stream=None) -> int:
+        """Reads and clears the device status word (bit 0: a bounded wait timed out)."""
+        v = L.UIN()
+        L.check(L.lib().gs_batch_status(self._h, C.byref(v), stream_handle(stream)),
+                "gs_batch_status")
+        return v.value
+
     def run(self, graph: bool = True, stream=None):
         f = L.lib().gs_batch_run_graph if graph else L.lib().gs_batch_run
         L.check(f(self._h, stream_handle(stream)), "gs_batch_run")

@@ -402,8 +402,9 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
  * to kpad_i = the next power of two: X_i row-major [ncols_i][kpad_i], Y_i [nrows_i][kpad_i],
  * 32-byte aligned (the padding columns of Y_i receive A_i times the padding of X_i). */
 typedef struct gs_batch gs_batch;
-/* Builds the work list (matrix, K1 unit, right-hand-side block), longest first; allocates
- * and synchronises.  Each matrix starts with one block of kpad_i columns. */
+/* Builds the work list (K1 units or row blocks of each matrix, per right-hand-side block),
+ * longest first; allocates and synchronises.  Each matrix starts with one block of kpad_i
+ * columns and the path GS_BATCH_AUTO. */
 gs_status gs_batch_create(gs_batch **out, UIN count, gs_matrix *const *mats, const UIN *k,
                           gs_stream stream);
 gs_status gs_batch_destroy(gs_batch *B);
@@ -418,6 +419,26 @@ gs_status gs_batch_set_operands(gs_batch *B, void *const *d_X, void *const *d_Y,
  * passes over A_i, each gathering kb_i values per stored element.  Rebuilds the work list
  * (and drops a captured graph). */
 gs_status gs_batch_set_blocking(gs_batch *B, const UIN *kb, gs_stream stream);
+/* How each matrix of a batch runs.  GS_BATCH_K1: warps over its K1 units, gathering X rows
+ * through L1 / L2.  GS_BATCH_BAND: thread blocks over blocks of consecutive rows, each
+ * staging its value and column segments and the rows of X its columns reach into shared
+ * memory (for banded matrices); the matrix's CSR arrays are rebuilt once from its K1
+ * layout (nnz (4 + value size) bytes more device memory).  GS_BATCH_AUTO (the default):
+ * row blocks when every row with its X band fits a block's shared memory at the current
+ * block width, else K1 units.  Both give the same bits. */
+#define GS_BATCH_AUTO 0u
+#define GS_BATCH_K1 1u
+#define GS_BATCH_BAND 2u
+/* Sets the requested path of every matrix and rebuilds the work list (drops a captured
+ * graph); GS_ERR_UNSUPPORTED (nothing changed) if a matrix held to GS_BATCH_BAND does not
+ * fit at its block width (gs_batch_set_blocking refuses such a width the same way). */
+gs_status gs_batch_set_paths(gs_batch *B, const UIN *path, gs_stream stream);
+/* The path each matrix runs on (GS_BATCH_K1 or GS_BATCH_BAND; array of count). */
+gs_status gs_batch_paths(const gs_batch *B, UIN *path);
+/* Reads and clears the batch's device status word (synchronises): bit 0 set when a row
+ * block's shared-memory copies did not arrive within the bounded wait (its products were
+ * not written). */
+gs_status gs_batch_status(gs_batch *B, UIN *flags, gs_stream stream);
 /* One run: a counter reset and one persistent kernel launch on `stream`. */
 gs_status gs_batch_run(gs_batch *B, gs_stream stream);
 /* The same run replayed from a CUDA graph captured on the first call. */

@@ -115,3 +115,89 @@ def test_batch_argument_errors():
     with pytest.raises(GSError, match="power of two"):
         B.set_blocking([3])
     B.close()
+
+
+def _banded_mats(dtype, rng, count, long_rows=False):
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    out = []
+    for i in range(count):
+        n = int(rng.integers(500, 30000))
+        row, col, val = matgen.banded(n, int(rng.integers(16, 257)), 5, 60,
+                                      seed=int(rng.integers(1 << 30)))
+        if long_rows and i == 0:  # rows past one kK1Split piece (128 elements)
+            row, col, val = case("mixed", rng)
+        ncols = max(len(row) - 1, int(col.max()) + 1 if len(col) else 1)
+        out.append(E.Matrix(row, col, val, ncols=ncols, fmt="K1", vtype=dtype))
+    return out
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_row_blocks_equal_k1_units(dtype):
+    """Row blocks (X band staged in shared memory) give the K1 bits: every width, every
+    blocking (contiguous X blocks by bulk copy, strided ones by plain loads)."""
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(11)
+    mats = _banded_mats(dtype, rng, 9, long_rows=True)
+    ks = [1, 2, 3, 5, 8, 13, 16, 31, 32]
+    B = E.Batch(mats, ks)
+    assert B.paths == ["band"] * len(mats)
+    X, Y = B.make_operands([rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)])
+    ref = [A.spmm(x) for A, x in zip(mats, X)]
+    for blocking in (B.kpad, [max(1, kp // 2) for kp in B.kpad], [1] * len(mats)):
+        B.set_blocking(blocking)
+        for graph in (False, True):
+            for y in Y:
+                y.fill_(float("nan"))
+            B.run(graph=graph)
+            torch.cuda.synchronize()
+            for i, (y, r) in enumerate(zip(Y, ref)):
+                assert torch.equal(y, r), (blocking[i], graph, i)
+    assert B.status() == 0
+    B.set_paths(["k1"] * len(mats))
+    assert B.paths == ["k1"] * len(mats)
+    for y in Y:
+        y.fill_(float("nan"))
+    B.run()
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, r)
+    B.close()
+
+
+def test_mixed_paths_and_refusal():
+    """A matrix whose row reaches too wide a band runs as K1 units under "auto" and is
+    refused under "band"; a mixed batch (both kernels) still gives the K1 bits."""
+    from gpu_spmv_b200 import GSError
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(12)
+    n = 60000
+    row = np.array([0, 2] + [2] * (n - 1), np.uint32)
+    col = np.array([0, n - 1], np.uint32)
+    wide = E.Matrix(row, col, np.array([1.5, -2.0]), ncols=n, fmt="K1", vtype="f32")
+    mats = [wide] + _banded_mats("f32", rng, 3)
+    ks = [32, 32, 7, 1]
+    B = E.Batch(mats, ks)
+    assert B.paths == ["k1", "band", "band", "band"]
+    X, Y = B.make_operands([rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)])
+    ref = [A.spmm(x) for A, x in zip(mats, X)]
+    B.run()
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, r)
+    with pytest.raises(GSError, match="shared memory"):
+        B.set_paths(["band"] * 4)
+    assert B.paths == ["k1", "band", "band", "band"]  # unchanged after the refusal
+    B.set_paths(["auto", "auto", "k1", "band"])
+    assert B.paths == ["k1", "band", "k1", "band"]
+    for y in Y:
+        y.fill_(float("nan"))
+    B.run()
+    torch.cuda.synchronize()
+    for y, r in zip(Y, ref):
+        assert torch.equal(y, r)
+    assert B.status() == 0
+    B.close()
