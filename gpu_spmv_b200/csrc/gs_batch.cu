@@ -207,29 +207,68 @@ __device__ __forceinline__ void lds4(const double *p, double (&v)[4])
     v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
 }
 
+// Two FP32 sums at once (sm_100 packed f32x2 add): each half rounds exactly as the scalar
+// add.rn.  The products stay scalar mul.rn: ptxas contracts a packed multiply feeding a
+// packed add into a fused multiply-add, which would change the bits.
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b)
+{
+    float2 d;
+    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+        " add.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+// acc[k] = acc[k] + v x[k] for k < V, multiply and add rounded separately
+template <class T, int V>
+__device__ __forceinline__ void madd_row(T (&acc)[V], T v, const T (&x)[V])
+{
+    if constexpr (std::is_same<T, float>::value && V % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            const float2 p = make_float2(__fmul_rn(v, x[k]), __fmul_rn(v, x[k + 1]));
+            const float2 r = add2_rn(make_float2(acc[k], acc[k + 1]), p);
+            acc[k] = r.x;
+            acc[k + 1] = r.y;
+        }
+    } else {
+        using A = mm::Arith<T>;
+#pragma unroll
+        for (int k = 0; k < V; k++) acc[k] = A::add(acc[k], A::mul(v, x[k]));
+    }
+}
+
+// The dynamic shared memory of the row-block kernel (named here so that every access in the
+// non-inlined block function is known to be a shared-memory one)
+extern __shared__ __align__(128) unsigned char g_band_smem[];
+
 // The rows of a staged block, K right-hand sides: P lanes per row (16 bytes of the row's K
 // values each, or one lane for rows under 16 bytes), rows taken in the block's order (longest
 // first) round-robin by the lane groups, so the rows of a warp have similar lengths.  Each
 // row sums its products in element order, restarting every kK1Split elements and adding the
-// pieces in order, as the K1 kernels do.
+// pieces in order, as the K1 kernels do.  sxo, svo, sco, sio: byte offsets in shared memory
+// of X row lo, the value and column segments and the row infos.
 template <class T, int K>
 __device__ __forceinline__ void band_rows(const BandArgs &m, uint32_t row0, uint32_t nr,
-                                          uint32_t lo, const T *sx, const T *sv,
-                                          const uint32_t *sc, const uint2 *sinfo, uint32_t off)
+                                          uint32_t lo, uint32_t svo, uint32_t sco,
+                                          uint32_t sio, uint32_t off)
 {
     using A = mm::Arith<T>;
     constexpr int P = (K * (int)sizeof(T) >= 16) ? K * (int)sizeof(T) / 16 : 1;
     constexpr int V = K / P;
     constexpr int G = kBandThreads / P;
+    constexpr uint32_t rowb = K * sizeof(T);
     const int grp = (int)threadIdx.x / P, pl = (int)threadIdx.x % P;
     T *__restrict__ y = static_cast<T *>(m.yout) + off + pl * V;
-    const T *sxl = sx + pl * V;
+    // X row c at byte xo + c * rowb (modulo 2^32: xo wraps below zero for lo > 0)
+    const uint32_t xo = (uint32_t)(pl * V * (int)sizeof(T)) - lo * rowb;
+    const uint2 *sinfo = reinterpret_cast<const uint2 *>(g_band_smem + sio);
 #pragma unroll 1
     for (uint32_t i = (uint32_t)grp; i < nr; i += G) {
         const uint2 inf = sinfo[i];
-        const T *rv = sv + (inf.x & 0xffffu);
-        const uint32_t *rc = sc + (inf.x & 0xffffu);
-        const uint32_t len = inf.y;
+        const uint32_t st = inf.x & 0xffffu, len = inf.y;
+        const T *rv = reinterpret_cast<const T *>(g_band_smem + svo) + st;
+        const uint32_t *rc = reinterpret_cast<const uint32_t *>(g_band_smem + sco) + st;
         T tot[V];
 #pragma unroll 1
         for (uint32_t p0 = 0;; p0 += kK1Split) {
@@ -237,21 +276,29 @@ __device__ __forceinline__ void band_rows(const BandArgs &m, uint32_t row0, uint
 #pragma unroll
             for (int k = 0; k < V; k++) acc[k] = T(0);
             const uint32_t pe = min(len, p0 + kK1Split);
+            uint32_t j = p0;
 #pragma unroll 1
-            for (uint32_t j = p0; j < pe; j += kBandPad) {
+            for (; j + kBandPad <= pe; j += kBandPad) {
                 T v[4], xv[4][V];
                 lds4(rv + j, v);
                 const uint4 c4 = *reinterpret_cast<const uint4 *>(rc + j);
-                const uint32_t c[4] = {c4.x - lo, c4.y - lo, c4.z - lo, c4.w - lo};
+                const uint32_t c[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
-                for (int b = 0; b < 4; b++) {
-                    if (j + b < pe) lds_vec<T, V>(sxl + (size_t)c[b] * K, xv[b]);
-                }
+                for (int b = 0; b < 4; b++)
+                    lds_vec<T, V>(reinterpret_cast<const T *>(g_band_smem + (xo + c[b] * rowb)), xv[b]);
 #pragma unroll
-                for (int b = 0; b < 4; b++) {
+                for (int b = 0; b < 4; b++) madd_row<T, V>(acc, v[b], xv[b]);
+            }
+            if (j < pe) {  // the last 1-3 elements
+                T v[4], xv[4][V];
+                lds4(rv + j, v);
+                const uint4 c4 = *reinterpret_cast<const uint4 *>(rc + j);
+                const uint32_t c[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
                     if (j + b < pe) {
-#pragma unroll
-                        for (int k = 0; k < V; k++) acc[k] = A::add(acc[k], A::mul(v[b], xv[b][k]));
+                        lds_vec<T, V>(reinterpret_cast<const T *>(g_band_smem + (xo + c[b] * rowb)), xv[b]);
+                        madd_row<T, V>(acc, v[b], xv[b]);
                     }
                 }
             }
@@ -267,9 +314,9 @@ __device__ __forceinline__ void band_rows(const BandArgs &m, uint32_t row0, uint
 // copies did not complete within the bounded wait; the status word then has bit 0 set.
 template <class T, int K>
 __device__ __noinline__ bool band_block(const BandArgs &m, uint32_t b, uint32_t rb,
-                                        unsigned char *smem, uint64_t *bar, uint32_t &phase,
-                                        uint32_t *status)
+                                        uint64_t *bar, uint32_t &phase, uint32_t *status)
 {
+    unsigned char *smem = g_band_smem;
     const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + b));
     const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + b) + 1);
     const uint32_t row0 = q0.x, row1 = q0.y, lo = q0.z, hi = q0.w, e0 = q1.x, e1 = q1.y;
@@ -279,14 +326,14 @@ __device__ __noinline__ bool band_block(const BandArgs &m, uint32_t b, uint32_t 
     const size_t i0 = ((size_t)row0 * 8) & ~size_t(15);
     const bool xbulk = m.xbulk != 0;
     const uint32_t tx = (uint32_t)(nb.v + nb.c + nb.i + (xbulk ? nb.x : 0));
-    unsigned char *s_v = smem + nb.x, *s_c = s_v + nb.v, *s_i = s_c + nb.c;
+    const uint32_t svo = (uint32_t)nb.x, sco = svo + (uint32_t)nb.v, sio = sco + (uint32_t)nb.c;
     if (threadIdx.x == 0 && tx) {
         bulk::mbar_expect_tx(bar, tx);
         if (nb.v)
-            bulk::bulk_g2s(s_v, static_cast<const T *>(m.val) + e0, (uint32_t)nb.v, bar);
-        if (nb.c) bulk::bulk_g2s(s_c, m.col + e0, (uint32_t)nb.c, bar);
+            bulk::bulk_g2s(smem + svo, static_cast<const T *>(m.val) + e0, (uint32_t)nb.v, bar);
+        if (nb.c) bulk::bulk_g2s(smem + sco, m.col + e0, (uint32_t)nb.c, bar);
         if (nb.i)
-            bulk::bulk_g2s(s_i, reinterpret_cast<const unsigned char *>(m.info) + i0,
+            bulk::bulk_g2s(smem + sio, reinterpret_cast<const unsigned char *>(m.info) + i0,
                            (uint32_t)nb.i, bar);
         if (xbulk && nb.x)
             bulk::bulk_g2s(smem, static_cast<const T *>(m.xin) + (size_t)lo * K, (uint32_t)nb.x,
@@ -304,7 +351,7 @@ __device__ __noinline__ bool band_block(const BandArgs &m, uint32_t b, uint32_t 
         for (uint32_t q = threadIdx.x; q < total; q += kBandThreads) {
             const uint32_t row = q / upr, part = q % upr;
             const unsigned char *src = xg + (size_t)row * gstride + part * u;
-            unsigned char *dst = smem + (size_t)row * rowb + part * u;
+            unsigned char *dst = smem + row * (uint32_t)rowb + part * u;
             if constexpr (u == 16) *reinterpret_cast<uint4 *>(dst) = __ldg(reinterpret_cast<const uint4 *>(src));
             else if constexpr (u == 8) *reinterpret_cast<uint2 *>(dst) = __ldg(reinterpret_cast<const uint2 *>(src));
             else *reinterpret_cast<uint32_t *>(dst) = __ldg(reinterpret_cast<const uint32_t *>(src));
@@ -319,9 +366,7 @@ __device__ __noinline__ bool band_block(const BandArgs &m, uint32_t b, uint32_t 
         if (threadIdx.x == 0) atomicOr(status, 1u);
         return false;
     }
-    band_rows<T, K>(m, row0, row1 - row0, lo, reinterpret_cast<const T *>(smem),
-                    reinterpret_cast<const T *>(s_v), reinterpret_cast<const uint32_t *>(s_c),
-                    reinterpret_cast<const uint2 *>(s_i + ((size_t)row0 * 8 - i0)), off);
+    band_rows<T, K>(m, row0, row1 - row0, lo, svo, sco, sio + (uint32_t)((size_t)row0 * 8 - i0), off);
     return true;
 }
 
@@ -332,7 +377,6 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_batch_band(
     const BandArgs *__restrict__ bdesc, const uint2 *__restrict__ items, uint32_t nitems,
     uint32_t *next, uint32_t *status)
 {
-    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t s_item;
     if (threadIdx.x == 0) {
@@ -351,12 +395,12 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_batch_band(
         const BandArgs &m = bdesc[mi];
         const uint32_t kb = m.ld / m.nrb;
         bool ok;
-        if (kb == 1) ok = band_block<T, 1>(m, w.y, rb, smem, &bar, phase, status);
-        else if (kb == 2) ok = band_block<T, 2>(m, w.y, rb, smem, &bar, phase, status);
-        else if (kb == 4) ok = band_block<T, 4>(m, w.y, rb, smem, &bar, phase, status);
-        else if (kb == 8) ok = band_block<T, 8>(m, w.y, rb, smem, &bar, phase, status);
-        else if (kb == 16) ok = band_block<T, 16>(m, w.y, rb, smem, &bar, phase, status);
-        else ok = band_block<T, 32>(m, w.y, rb, smem, &bar, phase, status);
+        if (kb == 1) ok = band_block<T, 1>(m, w.y, rb, &bar, phase, status);
+        else if (kb == 2) ok = band_block<T, 2>(m, w.y, rb, &bar, phase, status);
+        else if (kb == 4) ok = band_block<T, 4>(m, w.y, rb, &bar, phase, status);
+        else if (kb == 8) ok = band_block<T, 8>(m, w.y, rb, &bar, phase, status);
+        else if (kb == 16) ok = band_block<T, 16>(m, w.y, rb, &bar, phase, status);
+        else ok = band_block<T, 32>(m, w.y, rb, &bar, phase, status);
         if (!ok) return;
         // this item's shared-memory reads and writes precede the next item's bulk copies
         bulk::fence_proxy_async();
