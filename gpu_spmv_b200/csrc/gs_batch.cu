@@ -136,8 +136,10 @@ __global__ void __launch_bounds__(256) k_batch(const mm::MMArgs *__restrict__ de
 
 // ---------------------------------------------------------------------------------------
 // Row blocks with the X band in shared memory.
-constexpr int kBandThreads = 256;
-constexpr uint32_t kBandSmem = 110u * 1024u;  // dynamic shared memory per block: 2 per SM
+constexpr int kBandConsumers = 480;                   // 15 warps multiply
+constexpr int kBandThreads = kBandConsumers + 32;     // + 1 warp stages the blocks
+constexpr uint32_t kBandSmem = 110u * 1024u;          // shared memory per stage
+constexpr int kBandStages = 2;                        // one block per SM: 220 KB
 constexpr uint32_t kBandRowsMax = 4096;        // rows per block (< 2^16: packed in info)
 constexpr uint32_t kBandPad = 4;               // row segments start on multiples of 4 elements
 
@@ -247,21 +249,21 @@ extern __shared__ __align__(128) unsigned char g_band_smem[];
 // first) round-robin by the lane groups, so the rows of a warp have similar lengths.  Each
 // row sums its products in element order, restarting every kK1Split elements and adding the
 // pieces in order, as the K1 kernels do.  sxo, svo, sco, sio: byte offsets in shared memory
-// of X row lo, the value and column segments and the row infos.
+// of X row lo, the value and column segments and the row infos.  Consumer threads only.
 template <class T, int K>
 __device__ __forceinline__ void band_rows(const BandArgs &m, uint32_t row0, uint32_t nr,
-                                          uint32_t lo, uint32_t svo, uint32_t sco,
-                                          uint32_t sio, uint32_t off)
+                                          uint32_t lo, uint32_t sxo, uint32_t svo,
+                                          uint32_t sco, uint32_t sio, uint32_t off)
 {
     using A = mm::Arith<T>;
     constexpr int P = (K * (int)sizeof(T) >= 16) ? K * (int)sizeof(T) / 16 : 1;
     constexpr int V = K / P;
-    constexpr int G = kBandThreads / P;
+    constexpr int G = kBandConsumers / P;
     constexpr uint32_t rowb = K * sizeof(T);
     const int grp = (int)threadIdx.x / P, pl = (int)threadIdx.x % P;
     T *__restrict__ y = static_cast<T *>(m.yout) + off + pl * V;
     // X row c at byte xo + c * rowb (modulo 2^32: xo wraps below zero for lo > 0)
-    const uint32_t xo = (uint32_t)(pl * V * (int)sizeof(T)) - lo * rowb;
+    const uint32_t xo = sxo + (uint32_t)(pl * V * (int)sizeof(T)) - lo * rowb;
     const uint2 *sinfo = reinterpret_cast<const uint2 *>(g_band_smem + sio);
 #pragma unroll 1
     for (uint32_t i = (uint32_t)grp; i < nr; i += G) {
@@ -310,101 +312,176 @@ __device__ __forceinline__ void band_rows(const BandArgs &m, uint32_t row0, uint
     }
 }
 
-// One row block: stage, then multiply.  Returns false (in every thread) when the staging
-// copies did not complete within the bounded wait; the status word then has bit 0 set.
-template <class T, int K>
-__device__ __noinline__ bool band_block(const BandArgs &m, uint32_t b, uint32_t rb,
-                                        uint64_t *bar, uint32_t &phase, uint32_t *status)
+// Plan of one staged item, written by the producer before it arrives on the stage's full
+// barrier (whose completion makes it visible to the consumers).
+struct BandStage {
+    uint32_t valid, mi, rb, row0, nr, lo, hi;
+    uint32_t svo, sco, sio;  // byte offsets in the stage buffer
+};
+
+// Producer, before its stage is free: item w's descriptors and copy sizes.
+struct BandPlan {
+    BandStage st;
+    const void *val, *col, *info, *x;
+    uint32_t e0, nv, nc, ni, nx;  // nx: bytes of X by bulk copy (0: none or plain loads)
+    size_t i0;
+};
+template <class T>
+__device__ __forceinline__ BandPlan band_plan(const BandArgs *__restrict__ bdesc, uint2 w)
 {
-    unsigned char *smem = g_band_smem;
-    const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + b));
-    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + b) + 1);
+    BandPlan p;
+    const uint32_t mi = w.x >> 5, rb = w.x & 31u;
+    const BandArgs &m = bdesc[mi];
+    const uint32_t K = m.ld / m.nrb;
+    const uint4 q0 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + w.y));
+    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(m.blocks + w.y) + 1);
     const uint32_t row0 = q0.x, row1 = q0.y, lo = q0.z, hi = q0.w, e0 = q1.x, e1 = q1.y;
-    const uint32_t off = rb * K;
+    const BandBytes nb = band_bytes(lo, hi, e0, e1, row0, row1, (size_t)K * sizeof(T), sizeof(T));
+    p.i0 = ((size_t)row0 * 8) & ~size_t(15);
+    p.st.valid = 1;
+    p.st.mi = mi;
+    p.st.rb = rb;
+    p.st.row0 = row0;
+    p.st.nr = row1 - row0;
+    p.st.lo = lo;
+    p.st.hi = hi;
+    p.st.svo = (uint32_t)nb.x;
+    p.st.sco = p.st.svo + (uint32_t)nb.v;
+    p.st.sio = p.st.sco + (uint32_t)nb.c;
+    p.val = static_cast<const T *>(m.val) + e0;
+    p.col = m.col + e0;
+    p.info = reinterpret_cast<const unsigned char *>(m.info) + p.i0;
+    p.x = static_cast<const T *>(m.xin) + (size_t)lo * K;
+    p.e0 = e0;
+    p.nv = (uint32_t)nb.v;
+    p.nc = (uint32_t)nb.c;
+    p.ni = (uint32_t)nb.i;
+    p.nx = m.xbulk ? (uint32_t)nb.x : 0u;
+    return p;
+}
+// Producer, once the stage is free: the plan -> st, the bulk copies into stage buffer `buf`
+// (values, columns, row infos, and X rows lo..hi-1 when contiguous), completing on `full`.
+__device__ __forceinline__ void band_arm(const BandPlan &p, BandStage &st, uint32_t buf,
+                                         uint64_t *full)
+{
+    st = p.st;
+    st.sio = p.st.sio + (uint32_t)((size_t)p.st.row0 * 8 - p.i0);
+    unsigned char *b = g_band_smem + buf;
+    bulk::mbar_expect_tx(full, p.nv + p.nc + p.ni + p.nx);  // the producer's arrival too
+    if (p.nv) bulk::bulk_g2s(b + p.st.svo, p.val, p.nv, full);
+    if (p.nc) bulk::bulk_g2s(b + p.st.sco, p.col, p.nc, full);
+    if (p.ni) bulk::bulk_g2s(b + p.st.sio, p.info, p.ni, full);
+    if (p.nx) bulk::bulk_g2s(b, p.x, p.nx, full);
+}
+
+// Consumers: one staged item (its copies complete), K right-hand sides.
+template <class T, int K>
+__device__ __noinline__ void band_item(const BandArgs &m, const BandStage &st, uint32_t buf)
+{
+    const uint32_t off = st.rb * K;
     constexpr size_t rowb = K * sizeof(T);
-    const BandBytes nb = band_bytes(lo, hi, e0, e1, row0, row1, rowb, sizeof(T));
-    const size_t i0 = ((size_t)row0 * 8) & ~size_t(15);
-    const bool xbulk = m.xbulk != 0;
-    const uint32_t tx = (uint32_t)(nb.v + nb.c + nb.i + (xbulk ? nb.x : 0));
-    const uint32_t svo = (uint32_t)nb.x, sco = svo + (uint32_t)nb.v, sio = sco + (uint32_t)nb.c;
-    if (threadIdx.x == 0 && tx) {
-        bulk::mbar_expect_tx(bar, tx);
-        if (nb.v)
-            bulk::bulk_g2s(smem + svo, static_cast<const T *>(m.val) + e0, (uint32_t)nb.v, bar);
-        if (nb.c) bulk::bulk_g2s(smem + sco, m.col + e0, (uint32_t)nb.c, bar);
-        if (nb.i)
-            bulk::bulk_g2s(smem + sio, reinterpret_cast<const unsigned char *>(m.info) + i0,
-                           (uint32_t)nb.i, bar);
-        if (xbulk && nb.x)
-            bulk::bulk_g2s(smem, static_cast<const T *>(m.xin) + (size_t)lo * K, (uint32_t)nb.x,
-                           bar);
-    }
-    if (!xbulk && hi > lo) {
+    if (m.xbulk == 0 && st.hi > st.lo) {
         // strided or narrow X block: plain loads, 16 bytes (or the whole row) per thread
         constexpr uint32_t u = rowb >= 16 ? 16 : (uint32_t)rowb;
         constexpr uint32_t upr = (uint32_t)rowb / u;
-        const uint32_t total = (hi - lo) * upr;
+        const uint32_t total = (st.hi - st.lo) * upr;
         const unsigned char *xg = static_cast<const unsigned char *>(m.xin) +
-                                  ((size_t)lo * m.ld + off) * sizeof(T);
+                                  ((size_t)st.lo * m.ld + off) * sizeof(T);
         const size_t gstride = (size_t)m.ld * sizeof(T);
+        unsigned char *sb = g_band_smem + buf;
 #pragma unroll 4
-        for (uint32_t q = threadIdx.x; q < total; q += kBandThreads) {
+        for (uint32_t q = threadIdx.x; q < total; q += kBandConsumers) {
             const uint32_t row = q / upr, part = q % upr;
             const unsigned char *src = xg + (size_t)row * gstride + part * u;
-            unsigned char *dst = smem + row * (uint32_t)rowb + part * u;
+            unsigned char *dst = sb + row * (uint32_t)rowb + part * u;
             if constexpr (u == 16) *reinterpret_cast<uint4 *>(dst) = __ldg(reinterpret_cast<const uint4 *>(src));
             else if constexpr (u == 8) *reinterpret_cast<uint2 *>(dst) = __ldg(reinterpret_cast<const uint2 *>(src));
             else *reinterpret_cast<uint32_t *>(dst) = __ldg(reinterpret_cast<const uint32_t *>(src));
         }
+        asm volatile("bar.sync 1, %0;" ::"n"(kBandConsumers) : "memory");  // consumers only
     }
-    bool ok = true;
-    if (tx) {
-        ok = bulk::mbar_wait_bounded(bar, phase);
-        phase ^= 1u;
-    }
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicOr(status, 1u);
-        return false;
-    }
-    band_rows<T, K>(m, row0, row1 - row0, lo, svo, sco, sio + (uint32_t)((size_t)row0 * 8 - i0), off);
-    return true;
+    band_rows<T, K>(m, st.row0, st.nr, st.lo, buf, buf + st.svo, buf + st.sco, buf + st.sio, off);
 }
 
-// Persistent thread blocks over a work list of row blocks (x = matrix << 5 | right-hand-
-// side block, y = row block), one item per block at a time.
+// Persistent, one block per SM over a work list of row blocks (x = matrix << 5 | right-hand-
+// side block, y = row block), warp-specialised: the last warp takes items from the atomic
+// counter and stages each into one of two shared-memory buffers with TMA bulk copies (full
+// barrier: copies and plan landed); the other 15 warps multiply the staged block and release
+// the buffer (empty barrier), so the next block's copies overlap this block's products.
+// Every wait is bounded (about 2 s): a timeout sets bit 0 of the status word, and the
+// producer waits (bounded) for the copies it issued before it leaves.
 template <class T>
-__global__ void __launch_bounds__(kBandThreads, 2) k_batch_band(
+__global__ void __launch_bounds__(kBandThreads, 1) k_batch_band(
     const BandArgs *__restrict__ bdesc, const uint2 *__restrict__ items, uint32_t nitems,
     uint32_t *next, uint32_t *status)
 {
-    __shared__ uint64_t bar;
-    __shared__ uint32_t s_item;
+    __shared__ uint64_t full[kBandStages], empty[kBandStages];
+    __shared__ BandStage st[kBandStages];
     if (threadIdx.x == 0) {
-        bulk::mbar_init(&bar, 1);
+        for (int i = 0; i < kBandStages; i++) {
+            bulk::mbar_init(&full[i], 1);
+            bulk::mbar_init(&empty[i], kBandConsumers / 32);
+        }
         bulk::fence_mbar_init();
     }
     __syncthreads();
-    uint32_t phase = 0;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(next, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
-        if (it >= nitems) return;
-        const uint2 w = items[it];
-        const uint32_t mi = w.x >> 5, rb = w.x & 31u;
-        const BandArgs &m = bdesc[mi];
+    if (threadIdx.x >= kBandConsumers) {
+        // producer: one lane
+        if (threadIdx.x != kBandConsumers) return;
+        uint32_t eph = 0;     // bit s: parity of stage s's empty barrier awaited next
+        uint32_t issued = 0;  // bit s: stage s has been armed (its copies may be in flight)
+        for (uint32_t k = 0;; k++) {
+            const int sidx = (int)(k & 1u);
+            // the next item's descriptors load while the consumers still use the stage
+            const uint32_t it = atomicAdd(next, 1u);
+            BandPlan p;
+            if (it < nitems) p = band_plan<T>(bdesc, items[it]);
+            if ((issued >> sidx) & 1u) {
+                if (!bulk::mbar_wait_bounded(&empty[sidx], (eph >> sidx) & 1u)) {
+                    atomicOr(status, 1u);
+                    // leave only once the copies issued earlier have landed (bounded): the
+                    // full barrier of stage t was armed last for phase (k - 2 + t') / 2
+                    for (int t = 0; t < kBandStages; t++) {
+                        const uint32_t last = (k - 1u - (uint32_t)((sidx + 1 + t) & 1)) >> 1;
+                        if ((issued >> t) & 1u) bulk::mbar_wait_bounded(&full[t], last & 1u);
+                    }
+                    return;
+                }
+                eph ^= 1u << sidx;
+            }
+            if (it >= nitems) {
+                st[sidx].valid = 0;
+                bulk::mbar_expect_tx(&full[sidx], 0);
+                return;
+            }
+            band_arm(p, st[sidx], (uint32_t)sidx * kBandSmem, &full[sidx]);
+            issued |= 1u << sidx;
+        }
+    }
+    // consumers
+    uint32_t fph = 0;  // bit s: parity of stage s's full barrier awaited next
+    for (uint32_t k = 0;; k++) {
+        const int sidx = (int)(k & 1u);
+        if (!bulk::mbar_wait_bounded(&full[sidx], (fph >> sidx) & 1u)) {
+            if ((threadIdx.x & 31) == 0) atomicOr(status, 1u);
+            return;
+        }
+        fph ^= 1u << sidx;
+        const BandStage &sp = st[sidx];
+        if (!sp.valid) return;
+        const BandArgs &m = bdesc[sp.mi];
         const uint32_t kb = m.ld / m.nrb;
-        bool ok;
-        if (kb == 1) ok = band_block<T, 1>(m, w.y, rb, &bar, phase, status);
-        else if (kb == 2) ok = band_block<T, 2>(m, w.y, rb, &bar, phase, status);
-        else if (kb == 4) ok = band_block<T, 4>(m, w.y, rb, &bar, phase, status);
-        else if (kb == 8) ok = band_block<T, 8>(m, w.y, rb, &bar, phase, status);
-        else if (kb == 16) ok = band_block<T, 16>(m, w.y, rb, &bar, phase, status);
-        else ok = band_block<T, 32>(m, w.y, rb, &bar, phase, status);
-        if (!ok) return;
-        // this item's shared-memory reads and writes precede the next item's bulk copies
+        const uint32_t buf = (uint32_t)sidx * kBandSmem;
+        if (kb == 1) band_item<T, 1>(m, sp, buf);
+        else if (kb == 2) band_item<T, 2>(m, sp, buf);
+        else if (kb == 4) band_item<T, 4>(m, sp, buf);
+        else if (kb == 8) band_item<T, 8>(m, sp, buf);
+        else if (kb == 16) band_item<T, 16>(m, sp, buf);
+        else band_item<T, 32>(m, sp, buf);
+        // this warp's reads (and plain writes) of the buffer precede its next bulk copies
         bulk::fence_proxy_async();
-        __syncthreads();
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) bulk::mbar_arrive(&empty[sidx]);
     }
 }
 
@@ -615,7 +692,7 @@ gs_status build_items(gs_batch *B, cudaStream_t s)
             for (uint32_t b = 0; b < (uint32_t)bm.hblocks.size(); b++) {
                 const BandBlock &blk = bm.hblocks[b];
                 const uint64_t e = blk.e1 - blk.e0;
-                const uint64_t cost = (e * P / kBandThreads + 1) * (V + 4) + (blk.row1 - blk.row0) / 8 +
+                const uint64_t cost = (e * P / kBandConsumers + 1) * (V + 4) + (blk.row1 - blk.row0) / 8 +
                                       (uint64_t)(blk.hi - blk.lo) * kb * vsize / 1024;
                 for (uint32_t rb = 0; rb < nrb; rb++)
                     bitems.push_back({cost, ((uint32_t)i << 5) | rb, b});
@@ -675,16 +752,17 @@ gs_status launch_batch(gs_batch *B, cudaStream_t s)
 template <class T>
 gs_status launch_band(gs_batch *B, cudaStream_t s)
 {
+    const uint32_t smem = kBandStages * kBandSmem;
     GS_CUDA(cudaFuncSetAttribute(k_batch_band<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kBandSmem));
+                                 (int)smem));
     int per_sm = 0, dev = 0, sms = 148;
     GS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_band<T>, kBandThreads,
-                                                          kBandSmem));
+                                                          smem));
     GS_CUDA(cudaGetDevice(&dev));
     GS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     B->bblocks = std::max(1, per_sm) * sms;
     GS_CUDA(cudaMemsetAsync(B->d_next.as<uint32_t>() + 1, 0, 4, s));
-    k_batch_band<T><<<B->bblocks, kBandThreads, kBandSmem, s>>>(
+    k_batch_band<T><<<B->bblocks, kBandThreads, smem, s>>>(
         B->d_bdesc.as<BandArgs>(), B->d_bitems.as<uint2>(), B->nbitems,
         B->d_next.as<uint32_t>() + 1, B->d_status.as<uint32_t>());
     GS_CHECK_LAUNCH();
