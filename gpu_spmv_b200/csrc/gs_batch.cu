@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) k_batch(const mm::MMArgs *__restrict__ de
 
 // ---------------------------------------------------------------------------------------
 // Row blocks with the X band in shared memory.
-constexpr int kBandConsumers = 480;                   // 15 warps multiply
+constexpr int kBandConsumers = 736;                   // 23 warps multiply
 constexpr int kBandThreads = kBandConsumers + 32;     // + 1 warp stages the blocks
 constexpr uint32_t kBandSmem = 110u * 1024u;          // shared memory per stage
 constexpr int kBandStages = 2;                        // one block per SM: 220 KB
