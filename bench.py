@@ -457,6 +457,40 @@ def time_batched(steps: int, count: int = 256):
     return out
 
 
+def pcie_bandwidth(hx, hy, dx, dy, reps: int = 10):
+    """GB/s of pinned host -> device and device -> host copies of these buffers, alone and
+    both at once (two streams), timed on the host around synchronised batches of copies."""
+    import torch
+
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(h2d, d2h):
+        for _ in range(2):
+            with torch.cuda.stream(s1):
+                if h2d:
+                    dx.copy_(hx, non_blocking=True)
+            with torch.cuda.stream(s2):
+                if d2h:
+                    hy.copy_(dy, non_blocking=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            with torch.cuda.stream(s1):
+                if h2d:
+                    dx.copy_(hx, non_blocking=True)
+            with torch.cuda.stream(s2):
+                if d2h:
+                    hy.copy_(dy, non_blocking=True)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    bx, by = hx.numel() * hx.element_size(), hy.numel() * hy.element_size()
+    t_in, t_out, t_both = run(True, False), run(False, True), run(True, True)
+    return {"h2d_gbs": round(bx / t_in / 1e9, 1), "d2h_gbs": round(by / t_out / 1e9, 1),
+            "h2d_gbs_concurrent": round(bx / t_both / 1e9, 1),
+            "d2h_gbs_concurrent": round(by / t_both / 1e9, 1)}
+
+
 def time_formats(row, col, val, x, steps: int):
     """µs per product of the other formats and of cuSPARSE CSR on the same matrix and x
     (per-launch CUDA events, mean over `steps` launches after warm-up)."""
@@ -689,7 +723,15 @@ def run_ours(args):
             t = torch.tensor([te, te_serial], dtype=torch.float64, device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             te, te_serial = float(t[0]), float(t[1])
+        # the link's ceiling for these copies: pinned host <-> device, both directions at
+        # once on two streams, as the streamed steps run them
+        pcie = pcie_bandwidth(hx, hy, dx, dy)
+        step_s = max(hx.element_size() * n / (pcie["h2d_gbs_concurrent"] * 1e9),
+                     hy.element_size() * n / (pcie["d2h_gbs_concurrent"] * 1e9))
+        ceiling = world * 2.0 * nnz / step_s / 1e9
         e2e = {"value": world * 2.0 * nnz * Ke / te / 1e9, "unit": "GFLOP/s",
+               "pcie": pcie, "pcie_ceiling": round(ceiling, 1),
+               "frac_of_pcie_ceiling": round(2.0 * nnz * Ke / te / 1e9 / (ceiling / world), 3),
                "h2d_bytes_per_step": hx.element_size() * n,
                "d2h_bytes_per_step": hy.element_size() * n, "steps": Ke,
                "path": "gs_spmv_host_stream (C ABI): per step, pinned host x -> device, "
