@@ -201,3 +201,46 @@ def test_mixed_paths_and_refusal():
         assert torch.equal(y, r)
     assert B.status() == 0
     B.close()
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_row_blocks_edge_matrices(dtype):
+    """Row blocks on edge shapes: no stored element, one row, one column, runs of empty
+    rows, rows past several kK1Split pieces and past a block's row limit; same bits as
+    the single-matrix product, empty rows written as zero."""
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    from mats import csr_from_lengths
+
+    rng = np.random.default_rng(21)
+    shapes = []
+    shapes.append((np.zeros(46, np.uint32), np.zeros(0, np.uint32), np.zeros(0), 45))
+    shapes.append(csr_from_lengths([300], 300, rng) + (300,))
+    row, col, val = csr_from_lengths(rng.integers(0, 2, 5000), 1, rng)
+    shapes.append((row, col, val, 1))
+    lens = rng.integers(0, 9, 9000)
+    lens[100:4500] = 0
+    row, col, val = csr_from_lengths(lens, 9000, rng)
+    shapes.append((row, col, val, 9000))
+    lens = rng.integers(1, 4, 700)
+    lens[[3, 350, 699]] = [520, 257, 700]
+    row, col, val = csr_from_lengths(lens, 700, rng)
+    shapes.append((row, col, val, 700))
+    row, col, val = matgen.banded(20000, 16, 1, 3, seed=5)  # short rows: blocks of 4096 rows
+    shapes.append((row, col, val, 20000))
+    mats = [E.Matrix(r, c, v, ncols=nc, fmt="K1", vtype=dtype) for r, c, v, nc in shapes]
+    ks = [4, 1, 8, 1, 3, 32]  # every row with its X band fits a stage at these widths
+    B = E.Batch(mats, ks)
+    assert B.paths == ["band"] * len(mats)
+    X, Y = B.make_operands([rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)])
+    ref = [A.spmm(x) for A, x in zip(mats, X)]
+    for y in Y:
+        y.fill_(float("nan"))
+    B.run()
+    torch.cuda.synchronize()
+    for (r, _, _, _), y, rf in zip(shapes, Y, ref):
+        assert torch.equal(y, rf)
+        assert torch.all(y[torch.from_numpy(np.diff(r.astype(np.int64)) == 0).cuda()] == 0)
+    assert B.status() == 0
+    B.close()
