@@ -110,38 +110,50 @@ __global__ void __launch_bounds__(256) k_fill(const FillArgs f)
     }
 }
 
-// one thread per sorted row g of chunk g/32: element e -> chp[c] + 32e + g%32
+// one warp per K1 work unit (a kK1Split-step piece of a 32-row chunk), lane = sorted row
+// g of the chunk: its elements e of the piece -> k1_slot(chp[c], nmc[c], e, g % 32); a chunk
+// of long rows is filled by as many warps as it has pieces
 template <class VIN, class VOUT>
-__global__ void k_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col,
+__global__ void k_fill_k1(uint32_t n, uint32_t units, const uint32_t *unit_chunk,
+                          const uint32_t *unit_base, const uint32_t *row, const uint32_t *col,
                           const VIN *val, const uint32_t *permi, const uint32_t *chp,
                           const uint32_t *nmc, bool blocked, VOUT *oval, uint32_t *ocol)
 {
-    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31u;
+    if (u >= units) return;
+    const uint32_t c = unit_chunk[u], j0 = (u - unit_base[c]) * kK1Split;
+    const uint32_t g = 32u * c + lane;
     if (g >= n) return;
     const uint32_t r = permi[g], b = row[r], len = row[r + 1] - b;
-    const uint32_t c = g / 32, cb = chp[c], m = nmc[c];
-    for (uint32_t e = 0; e < len; e++) {
-        const uint32_t pos = k1_slot(cb, m, e, g % 32, blocked);
+    const uint32_t cb = chp[c], m = nmc[c], j1 = min(len, j0 + kK1Split);
+    for (uint32_t e = j0; e < j1; e++) {
+        const uint32_t pos = k1_slot(cb, m, e, lane, blocked);
         oval[pos] = cvt<VIN, VOUT>(val[b + e]);
         ocol[pos] = col[b + e];
     }
 }
 
 template <class VIN>
-void launch_fill_k1(uint32_t n, const uint32_t *row, const uint32_t *col, const VIN *val,
-                    const uint32_t *permi, const uint32_t *chp, const uint32_t *nmc,
-                    bool blocked, gs_dtype vout, void *oval, uint32_t *ocol, cudaStream_t s)
+void launch_fill_k1(uint32_t n, uint32_t units, const uint32_t *unit_chunk,
+                    const uint32_t *unit_base, const uint32_t *row, const uint32_t *col,
+                    const VIN *val, const uint32_t *permi, const uint32_t *chp,
+                    const uint32_t *nmc, bool blocked, gs_dtype vout, void *oval, uint32_t *ocol,
+                    cudaStream_t s)
 {
-    const unsigned b = (n + 255) / 256;
+    if (!units) return;
+    const unsigned b = (units + 7) / 8;
     if (vout == GS_F64)
-        k_fill_k1<VIN, double><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc, blocked,
+        k_fill_k1<VIN, double><<<b, 256, 0, s>>>(n, units, unit_chunk, unit_base, row, col, val,
+                                                 permi, chp, nmc, blocked,
                                                  static_cast<double *>(oval), ocol);
     else if (vout == GS_F32)
-        k_fill_k1<VIN, float><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc, blocked,
+        k_fill_k1<VIN, float><<<b, 256, 0, s>>>(n, units, unit_chunk, unit_base, row, col, val,
+                                                permi, chp, nmc, blocked,
                                                 static_cast<float *>(oval), ocol);
     else
-        k_fill_k1<VIN, __nv_bfloat16><<<b, 256, 0, s>>>(n, row, col, val, permi, chp, nmc,
-                                                        blocked,
+        k_fill_k1<VIN, __nv_bfloat16><<<b, 256, 0, s>>>(n, units, unit_chunk, unit_base, row,
+                                                        col, val, permi, chp, nmc, blocked,
                                                         static_cast<__nv_bfloat16 *>(oval),
                                                         ocol);
 }
@@ -318,18 +330,22 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
         DevBuf col32;  // 32-bit columns before the 16-bit steps are taken
         if (u16) GS_TRY(col32.alloc_zero((size_t)A->lenVC * 4, s));
         uint32_t *ocol = u16 ? col32.as<uint32_t>() : A->col.as<uint32_t>();
-        // 16-bit steps: lane-blocked slot order (k1_slot); otherwise the reference's
-        if (val_type == GS_F64)
-            launch_fill_k1<double>(n, d_row, d_col, static_cast<const double *>(d_val),
-                                   A->permi.as<uint32_t>(), A->chp.as<uint32_t>(),
-                                   A->nmc.as<uint32_t>(), u16, p.vtype, A->val.p, ocol, s);
-        else
-            launch_fill_k1<float>(n, d_row, d_col, static_cast<const float *>(d_val),
-                                  A->permi.as<uint32_t>(), A->chp.as<uint32_t>(),
-                                  A->nmc.as<uint32_t>(), u16, p.vtype, A->val.p, ocol, s);
-        GS_CHECK_LAUNCH();
         GS_TRY(build_k1_plan(A->nmc.as<uint32_t>(), chunkNum, A->k1unit_chunk, A->k1unit_base,
                              A->k1partial, A->k1count, &A->k1units, s));
+        // 16-bit steps: lane-blocked slot order (k1_slot); otherwise the reference's
+        if (val_type == GS_F64)
+            launch_fill_k1<double>(n, A->k1units, A->k1unit_chunk.as<uint32_t>(),
+                                   A->k1unit_base.as<uint32_t>(), d_row, d_col,
+                                   static_cast<const double *>(d_val), A->permi.as<uint32_t>(),
+                                   A->chp.as<uint32_t>(), A->nmc.as<uint32_t>(), u16, p.vtype,
+                                   A->val.p, ocol, s);
+        else
+            launch_fill_k1<float>(n, A->k1units, A->k1unit_chunk.as<uint32_t>(),
+                                  A->k1unit_base.as<uint32_t>(), d_row, d_col,
+                                  static_cast<const float *>(d_val), A->permi.as<uint32_t>(),
+                                  A->chp.as<uint32_t>(), A->nmc.as<uint32_t>(), u16, p.vtype,
+                                  A->val.p, ocol, s);
+        GS_CHECK_LAUNCH();
         if (u16) {
             K1Args a{};
             a.nrows = n;
