@@ -211,6 +211,10 @@ gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32
 gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &P,
                             uint16_t *d_col16, cudaStream_t s);
 RowsArgs rows_args(const RowsPlan &P);
+// Baked layouts of whole [thw values | thw x] tiles per row (UNC tileH = 1, AXC), thw in
+// {4, 8, 16, 32}: a.val = ax, the plan built over tiles (its positions are tiles, its row
+// starts the first tile of each row; windows of 32 V tiles), y FP64.
+gs_status launch_tiles_baked(const RowsArgs &a, uint32_t thw, cudaStream_t s);
 gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
                       uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s);
 

@@ -594,6 +594,24 @@ static str_res run_baked(const char *name, UIN nrows, UIN nnz, const FPT *hax, U
 {
     DevBuf ax, y;
     gs::RowsPlan P;
+    if (!tiled && align == axw && (axw == 4 || axw == 8 || axw == 16 || axw == 32)) {
+        // whole [axw values | axw x] tiles per row (UNC tileH = 1, AXC): the tile kernel,
+        // its plan built over tiles (row r starts at tile rpos[r] / axw), in windows of one
+        // 32-tile chunk (a tile is 2 axw values: small matrices still get many warps)
+        DevBuf rtile;
+        if (h2d(ax, hax, lenAX) || y.alloc((size_t)nrows * 8) ||
+            rtile.alloc(((size_t)nrows + 1) * 4))
+            return error_res(name, gs_last_error());
+        k_div_table<<<(nrows + 256) / 256, 256>>>(nrows + 1, rpos.as<UIN>(), axw,
+                                                  rtile.as<UIN>());
+        if (gs::build_rows_plan(rtile.as<UIN>(), nullptr, nrows, 1, P, 0))
+            return error_res(name, gs_last_error());
+        gs::RowsArgs a = gs::rows_args(P);
+        a.val = ax.p;
+        a.y = y.p;
+        return timed(name, nrows, nnz, [&]() { return gs::launch_tiles_baked(a, axw, 0); }, y,
+                     ref);
+    }
     uint32_t V = tiled ? th : gs::kDirectV;
     bool aligned = false;
     if (tiled) aligned = align != 0 && (th == 2 || th == 4 || th == 8 || th == 16);

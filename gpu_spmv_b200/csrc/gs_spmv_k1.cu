@@ -97,11 +97,13 @@ __global__ void __launch_bounds__(256, std::is_same<VT, double>::value
     YT *__restrict__ y = static_cast<YT *>(a.y);
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    // no chunk cut into pieces: unit u is chunk u (one dependent load less per unit)
+    const bool whole = a.units == a.chunkNum;
     for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < a.units;
          u += warps) {
-        const uint32_t c = __ldg(a.unit_chunk + u);
-        const uint32_t ub = __ldg(a.unit_base + c);
-        const uint32_t np = __ldg(a.unit_base + c + 1) - ub;
+        const uint32_t c = whole ? u : __ldg(a.unit_chunk + u);
+        const uint32_t ub = whole ? u : __ldg(a.unit_base + c);
+        const uint32_t np = whole ? 1u : __ldg(a.unit_base + c + 1) - ub;
         const uint32_t piece = u - ub;
         const uint32_t nmc = __ldg(a.nmc + c);
         const uint32_t g = 32u * c + (uint32_t)lane;
@@ -160,10 +162,12 @@ __global__ void __launch_bounds__(256, std::is_same<VT, double>::value
             for (int k = 0; k < 8; k++) acc = k1_fma<VT, XT, AT>(acc, v[k], xv[k]);
         }
         // the last 1-7 slots of this lane.  FP32 / BF16 values with 32-bit columns: loads
-        // first, as one batch (5 % faster on the 27-point stencil); FP64 and 16-bit steps keep
-        // the plain loop, which measured faster for them
-        constexpr bool kBatchTail = !kDelta && !std::is_same<VT, double>::value;
-        for (; !kBatchTail && j < j1; j++) {
+        // first, as one batch (5 % faster on the 27-point stencil); FP64 the same when the
+        // whole chunk is shorter than 8 steps (its rows are all tail), else the plain loop,
+        // as for 16-bit steps, which measured faster for them
+        constexpr bool kF64 = std::is_same<VT, double>::value;
+        const bool batch_tail = !kDelta && (!kF64 || nmc < 8u);
+        for (; !batch_tail && j < j1; j++) {
             const uint32_t pos = base + 32u * j;
             uint32_t cj = (uint32_t)__ldcs(col + pos);
             if constexpr (kDelta) {
@@ -172,8 +176,8 @@ __global__ void __launch_bounds__(256, std::is_same<VT, double>::value
             }
             acc = k1_fma<VT, XT, AT>(acc, __ldcs(val + pos), __ldg(x + cj));
         }
-        constexpr int kTail = 7;
-        for (; kBatchTail && j < j1; j += kTail) {
+        constexpr int kTail = kF64 ? 4 : 7;  // FP64: 4 slots in its 32 registers
+        for (; batch_tail && j < j1; j += kTail) {
             const uint32_t rem = j1 - j;
             VT v[kTail];
             XT xv[kTail];

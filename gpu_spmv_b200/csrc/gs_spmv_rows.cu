@@ -1156,6 +1156,108 @@ __global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, uint32_t
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Baked layouts made of whole tiles per row (UNC tileH = 1: tiles of [THW values | THW x];
+// AXC: bricks of the same shape): the plan is built over tiles (a.npos = tiles, a.sbits =
+// first tile of each non-empty row), so one lane of a 32-tile chunk stands for one tile and
+// the striped segmented scan (stripe_chunk) adds tile sums into rows.  The tiles' values and
+// x are loaded cooperatively: in each of THW/2 load steps, groups of G = THW/2 lanes read 16
+// bytes of one tile's value half and the matching 16 bytes of its x half (both halves fully
+// coalesced across the warp), form two products, and sum them over the group (shuffle tree);
+// a shuffle transpose then hands tile k's sum to lane k.  Per tile: products in pairs, pairs
+// summed over a binary tree, fixed order.
+template <int THW, bool EMPTY>
+__global__ void __launch_bounds__(256) k_tiles_baked(const RowsArgs a)
+{
+    constexpr int G = THW / 2;      // lanes per tile in a load step
+    constexpr int TPI = 32 / G;     // tiles per load step
+    constexpr int NI = G;           // load steps per 32-tile chunk
+    const int lane = threadIdx.x & 31;
+    double *y = static_cast<double *>(a.y);
+    const double *ax = static_cast<const double *>(a.val);
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t cpwin = a.V;  // chunks per plan window
+    const unsigned lt = (1u << lane) - 1u;
+    if constexpr (EMPTY) {
+        for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
+            y[__ldg(a.empty + i)] = 0.0;
+    }
+    const uint32_t ntiles = a.npos;
+    const uint32_t nchunk = (ntiles + 31) / 32;
+    const int gl = lane % G, gt = lane / G;
+    // the sum of tile ch*32 + lane, in this lane (0 past the last tile)
+    auto chunk_sums = [&](uint32_t ch) -> double {
+        double part[NI];
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+            const uint32_t t = ch * 32u + (uint32_t)(i * TPI + gt);
+            part[i] = 0.0;
+            if (t < ntiles) {
+                const double *tp = ax + (size_t)t * (2 * THW) + 2 * gl;
+                const double2 v = __ldcs(reinterpret_cast<const double2 *>(tp));
+                const double2 xv = __ldcs(reinterpret_cast<const double2 *>(tp + THW));
+                part[i] = __dadd_rn(__dmul_rn(v.x, xv.x), __dmul_rn(v.y, xv.y));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+#pragma unroll
+            for (int d = G / 2; d >= 1; d >>= 1)
+                part[i] = __dadd_rn(part[i], __shfl_down_sync(kFull, part[i], d, G));
+        }
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+            const double v = __shfl_sync(kFull, part[i], (lane % TPI) * G);
+            if (lane / TPI == i) sum = v;
+        }
+        return sum;
+    };
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    for (uint32_t rg = gw; rg < nranges; rg += nwarps) {
+        const uint32_t c0 = rg * a.wpw * cpwin;
+        const uint32_t c1 = min(c0 + a.wpw * cpwin, nchunk);
+        uint32_t cnt = __ldg(a.wcount + rg * a.wpw);  // row starts before the range
+        bool seen = (c0 == 0);
+        double carry = 0.0;
+        for (uint32_t ch = c0; ch < c1; ch++) {
+            const uint32_t word = __ldg(a.sbits + ch);
+            const uint32_t vm =
+                ch * 32u + 32u <= ntiles ? 0xffffffffu : ((1u << (ntiles - ch * 32u)) - 1u);
+            const double prod = chunk_sums(ch);
+            stripe_chunk<double, double, double, EMPTY>(a, y, lane, lt, ch, nchunk, false, word,
+                                                        vm, prod, cnt, seen, carry);
+        }
+        // past the range: until the range's last row ends
+        if (seen) {
+            for (uint32_t ch = c1; ch < nchunk; ch++) {
+                const uint32_t word = __ldg(a.sbits + ch);
+                const uint32_t vm =
+                    ch * 32u + 32u <= ntiles ? 0xffffffffu : ((1u << (ntiles - ch * 32u)) - 1u);
+                const double prod = chunk_sums(ch);
+                if (!stripe_chunk<double, double, double, EMPTY>(a, y, lane, lt, ch, nchunk, true,
+                                                                 word, vm, prod, cnt, seen, carry))
+                    break;
+            }
+        }
+    }
+}
+
+template <int THW>
+gs_status launch_tiles_baked_t(const RowsArgs &a, cudaStream_t s)
+{
+    const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
+    uint32_t warps = nranges;
+    if (a.n_empty) warps = max(warps, min((a.n_empty + 31) / 32, 148u * 64u));
+    if (warps == 0) return GS_OK;
+    const uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
+    if (a.n_empty) k_tiles_baked<THW, true><<<blocks, 256, 0, s>>>(a);
+    else k_tiles_baked<THW, false><<<blocks, 256, 0, s>>>(a);
+    GS_CHECK_LAUNCH();
+    return GS_OK;
+}
+
 }  // namespace
 
 gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
@@ -1312,6 +1414,17 @@ gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtyp
 #undef GS_MIXED
     return fail(GS_ERR_UNSUPPORTED, "value type %d / index type %d not supported", (int)vtype,
                 (int)itype);
+}
+
+gs_status launch_tiles_baked(const RowsArgs &a, uint32_t thw, cudaStream_t s)
+{
+    switch (thw) {
+    case 4: return launch_tiles_baked_t<4>(a, s);
+    case 8: return launch_tiles_baked_t<8>(a, s);
+    case 16: return launch_tiles_baked_t<16>(a, s);
+    case 32: return launch_tiles_baked_t<32>(a, s);
+    default: return fail(GS_ERR_UNSUPPORTED, "tile half width %u (4, 8, 16 or 32)", thw);
+    }
 }
 
 }  // namespace gs

@@ -275,6 +275,12 @@ class Ref:
                     "ref_axt_dims": (None, [vp, _u32p]),
                     "ref_axt_copy": (None, [vp, _f64p, _u32p, _u32p]),
                     "ref_axt_free": (None, [vp]),
+                    "ref_gpu_csr": (C.c_double, [u32, u32, u32, _f64p, _u32p, _u32p, _f64p,
+                                                 _f64p, _f64p]),
+                    "ref_gpu_k1": (C.c_double, [vp, u32, _f64p, _f64p, _f64p]),
+                    "ref_gpu_axc": (C.c_double, [vp, u32, _f64p, _f64p]),
+                    "ref_gpu_axt_uh": (C.c_double, [vp, u32, u32, _f64p, _f64p]),
+                    "ref_gpu_axt_uh1hw16": (C.c_double, [vp, u32, u32, _f64p, _f64p]),
                 }
                 for name, (res, args) in sig.items():
                     f = getattr(lib, name)
@@ -372,6 +378,44 @@ class Ref:
         out["fd"] = fd
         out["name"] = name.value.decode()
         self.lib.ref_axt_copy(h, out["ax"], out["sec"], out["con"])
+        self.lib.ref_axt_free(h)
+        return out
+
+
+    # ---- the reference's own GPU products (its kernels compiled for sm_100a; GPU needed)
+    def gpu_products(self, row, col, val, x, ref, cbs=256, tpw=4, th=4, reps=5):
+        """Device seconds of one launch (median of `reps` calls) of the reference's gcsr,
+        gk1, gaxc (hbs 32), gaxtuh (tileH th, tileHW 32, tpw tiles per warp) and gaxtuh1hw16w
+        (tileH 1, tileHW 16, 128 slots per warp) on this matrix, and each one's get_errors
+        summary against `ref`.  x is baked into the AXC / AXT layouts, as the reference does.
+        The matrix must have no all-empty 32-row chunk (gk1 reads a chunk's first slot
+        unconditionally)."""
+        import statistics
+
+        row, col, val, x, ref = _u32(row), _u32(col), _f64(val), _f64(x), _f64(ref)
+        n, nnz = len(row) - 1, int(row[-1])
+        out = {}
+
+        def run(name, fn):
+            ts, err = [], np.zeros(3, np.float64)
+            for _ in range(reps):
+                ts.append(fn(err))
+            out[name] = dict(seconds=statistics.median(ts), aErr=err[0], rErr=err[1])
+
+        run("gcsr", lambda e: self.lib.ref_gpu_csr(cbs, n, nnz, val, col, row, x, ref, e))
+        fd = np.zeros(3, np.float64)
+        h = self.lib.ref_k1(n, nnz, val, col, row, x, fd)
+        run("gk1", lambda e: self.lib.ref_gpu_k1(h, cbs, x, ref, e))
+        self.lib.ref_k1_free(h)
+        threads = os.cpu_count() or 1
+        h = self.lib.ref_axc(threads, 32, n, nnz, val, col, row, x, fd)
+        run("gaxc", lambda e: self.lib.ref_gpu_axc(h, cbs, ref, e))
+        self.lib.ref_axc_free(h)
+        h = self.lib.ref_axt(threads, 256, 32, th, b"UNC", n, nnz, val, col, row, x, fd, None)
+        run(f"gaxtuh{th}", lambda e: self.lib.ref_gpu_axt_uh(h, tpw, cbs, ref, e))
+        self.lib.ref_axt_free(h)
+        h = self.lib.ref_axt(threads, 256, 16, 1, b"UNC", n, nnz, val, col, row, x, fd, None)
+        run("gaxtuh1hw16", lambda e: self.lib.ref_gpu_axt_uh1hw16(h, 128, cbs, ref, e))
         self.lib.ref_axt_free(h)
         return out
 

@@ -14,6 +14,8 @@
  *   ref_k1_*           -> getFormatDataK1    (cudaSpmv.cu:782-846)
  *   ref_axc_*          -> getFormatDataAXC   (cudaSpmv.cu:1004-1062)
  *   ref_axt_*          -> getFormatDataAXT   (cudaSpmv.cu:1391-1566)
+ *   ref_gpu_*          -> test_gcsr, test_gk1, test_gaxc, test_gaxtuh, test_gaxtuh1hw16w
+ *                         (the reference's own GPU products, cudaSpmv.cu:547-2037)
  *
  * No reference code is copied here: the wrappers only marshal arguments into the
  * reference's own structs (str_matCSR, str_matK1, str_matAXC, str_matAXT) and back out.
@@ -193,6 +195,47 @@ void ref_axt_free(void *h)
 {
     str_matAXT *a = (str_matAXT *)h;
     free(a->ax); free(a->sec); free(a->con); free(a);
+}
+
+/* ---------------- the reference's own GPU products, compiled for sm_100a ----------------
+ * Each runs the reference's test function (device buffers, one launch timed by its cudaEvents
+ * (NUM_ITE = 1), result copied back, buffers freed) and returns its str_res: et (seconds)
+ * and the get_errors summary against `ref` in err3 = {aErr, rErr, pos}.  Only matrices
+ * without all-empty 32-row chunks may go to gk1: its first load of a chunk
+ * (cudaSpmv.cu:861) is unconditional. */
+static double res_out(const str_res &r, double *err3)
+{
+    err3[0] = r.sErr.aErr;
+    err3[1] = r.sErr.rErr;
+    err3[2] = (double)r.sErr.pos;
+    return r.et;
+}
+double ref_gpu_csr(UIN cbs, UIN nrows, UIN nnz, const FPT *val, const UIN *col,
+                   const UIN *row, const FPT *vec, const FPT *ref, double *err3)
+{
+    UIN *rl = (UIN *)malloc((size_t)(nrows ? nrows : 1) * sizeof(UIN));
+    str_matCSR m = make_csr(nrows, nnz, val, col, row, rl);
+    const str_res r = test_gcsr(cbs, m, vec, ref);             /* cudaSpmv.cu:547 */
+    free(rl);
+    return res_out(r, err3);
+}
+double ref_gpu_k1(void *h, UIN cbs, const FPT *vec, const FPT *ref, double *err3)
+{
+    return res_out(test_gk1(cbs, *(str_matK1 *)h, vec, ref), err3);    /* cudaSpmv.cu:871 */
+}
+double ref_gpu_axc(void *h, UIN cbs, const FPT *ref, double *err3)
+{
+    return res_out(test_gaxc(cbs, *(str_matAXC *)h, ref), err3);       /* cudaSpmv.cu:1100 */
+}
+/* tileH > 1, tileHW 32 */
+double ref_gpu_axt_uh(void *h, UIN tpw, UIN cbs, const FPT *ref, double *err3)
+{
+    return res_out(test_gaxtuh(tpw, cbs, *(str_matAXT *)h, ref), err3); /* cudaSpmv.cu:1963 */
+}
+/* tileH 1, tileHW 16; wpw / 32 tiles per warp must be even (the kernel takes tiles in pairs) */
+double ref_gpu_axt_uh1hw16(void *h, UIN wpw, UIN cbs, const FPT *ref, double *err3)
+{
+    return res_out(test_gaxtuh1hw16w(wpw, cbs, *(str_matAXT *)h, ref), err3); /* :1603 */
 }
 
 }  // extern "C"
