@@ -457,6 +457,58 @@ def time_batched(steps: int, count: int = 256):
     return out
 
 
+def time_dropin(workload: str, steps: int):
+    """The drop-in API the way the reference's main() drives it (cudaSpmv.cu:2319-2417): per
+    format, its getFormatData* converter (the reference's layouts, x baked into AXC / AXT as
+    the reference does) and its test_* entry point, `steps` launches (gs_set_num_ite).  Each
+    row: the converter's mfp / beta / conversion seconds and the product's mean device time,
+    with the reference's error summary against the drop-in ncsr (on the GPU here)."""
+    import ctypes as Cc
+
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import refapi as R
+
+    row, col, val, x = make_matrix(workload, 0)
+    n = len(row) - 1
+    lib = L.lib()
+    lib.gs_set_num_ite(max(1, steps))
+    h = R.csr_struct(row, col, val, name=workload + ".bin")
+    y_ref = np.zeros(n)
+    lib.ncsr(os.cpu_count() or 1, h.s, R.f64p(x), R.f64p(y_ref))
+    out = {}
+
+    def put(fd, res):
+        out[res.name.decode()] = dict(
+            format=fd.name.decode() if fd is not None else "fcsr", mfp=fd.mfp if fd else None,
+            beta=fd.beta if fd else None, conversion_s=fd.ct if fd else None,
+            us=round(res.et * 1e6, 2), gflops=round(res.flops / 1e9, 1),
+            abs_err=res.sErr.aErr, rel_err=res.sErr.rErr)
+
+    put(None, lib.test_gcsr(256, h.s, R.f64p(x), R.f64p(y_ref)))
+    k = L.StrMatK1()
+    fd = lib.getFormatDataK1(32, h.s, R.f64p(x), Cc.byref(k))
+    put(fd, lib.test_gk1(256, k, R.f64p(x), R.f64p(y_ref)))
+    R.free_struct_arrays(k, ("permi", "nmc", "chp", "val", "col"))
+    a = L.StrMatAXC()
+    fd = lib.getFormatDataAXC(os.cpu_count() or 1, 32, h.s, R.f64p(x), Cc.byref(a))
+    put(fd, lib.test_gaxc(256, a, R.f64p(y_ref)))
+    R.free_struct_arrays(a, ("ax", "brp", "mapx"))
+    for mode, th, thw, fn in (("UNC", 1, 16, lambda t: lib.test_gaxtuh1hw16w(128, 256, t, R.f64p(y_ref))),
+                              ("UNC", 1, 8, lambda t: lib.test_gaxtuh1hw08w(64, 256, t, R.f64p(y_ref))),
+                              ("UNC", 1, 4, lambda t: lib.test_gaxtuh1hw04w(32, 256, t, R.f64p(y_ref))),
+                              ("UNC", 4, 32, lambda t: lib.test_gaxtuh(4, 256, t, R.f64p(y_ref))),
+                              ("UNC", 8, 32, lambda t: lib.test_gaxtuh(4, 256, t, R.f64p(y_ref))),
+                              ("COM", 1, 32, lambda t: lib.test_gaxtch1(256, t, R.f64p(y_ref)))):
+        t = L.StrMatAXT()
+        fd = lib.getFormatDataAXT(os.cpu_count() or 1, 256, thw, th, mode.encode(), h.s,
+                                  R.f64p(x), Cc.byref(t))
+        put(fd, fn(t))
+        R.free_struct_arrays(t, ("ax", "sec", "con"))
+    lib.gs_set_num_ite(250)
+    return {"workload": WORKLOADS[workload]["desc"], "launches_per_entry_point": steps,
+            "entry_points": out}
+
+
 def pcie_bandwidth(hx, hy, dx, dy, reps: int = 10):
     """GB/s of pinned host -> device and device -> host copies of these buffers, alone and
     both at once (two streams), timed on the host around synchronised batches of copies."""
@@ -815,8 +867,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--only", choices=["mixed", "adjoint", "batched", "batched-small"],
-                    help="run one extension section alone and print its object")
+    ap.add_argument("--only", choices=["mixed", "adjoint", "batched", "batched-small", "dropin"],
+                    help="run one section alone and print its object (dropin: the reference's "
+                         "converters and test_* entry points, through this library, on --workload)")
     ap.add_argument("--format-steps", type=int, default=200)
     ap.add_argument("--no-clocks", action="store_true")
     args = ap.parse_args()
@@ -831,7 +884,8 @@ def main():
         fn = {"mixed": lambda: time_mixed(args.steps),
               "adjoint": lambda: time_adjoint(args.steps),
               "batched": lambda: time_batched(args.steps),
-              "batched-small": lambda: time_batched(args.steps, count=32)}[args.only]
+              "batched-small": lambda: time_batched(args.steps, count=32),
+              "dropin": lambda: time_dropin(args.workload, args.steps)}[args.only]
         print(json.dumps({args.only: fn()}))
         return 0
     return run_ours(args)
