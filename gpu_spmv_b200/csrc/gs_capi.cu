@@ -176,6 +176,16 @@ gs_status gs_spmv(const gs_matrix *A, const void *d_x, gs_dtype xtype, void *d_y
     if (f64 && xtype != GS_F64) return gs::fail(GS_ERR_UNSUPPORTED, "FP64 matrices take FP64 x");
     if (!f64 && xtype != GS_F32)
         return gs::fail(GS_ERR_UNSUPPORTED, "FP32/BF16 matrices take FP32 x");
+    if (A->tile_w && f64 && ytype == GS_F64 && !(flags & (GS_FLAG_STRIPED | GS_FLAG_TMA))) {
+        // whole tiles per row (UNC tileH = 1, AXC): the tile kernel over the tile plan
+        gs::RowsArgs t = gs::rows_args(A->tplan);
+        t.val = A->val.p;
+        t.col = A->col.p;
+        t.x = d_x;
+        t.y = d_y;
+        t.rbits = A->plan.padded ? A->plan.rbits.as<uint32_t>() : nullptr;
+        return gs::launch_tiles(t, A->tile_w, false, s);
+    }
     gs::RowsArgs a = gs::rows_args(A->plan);
     a.val = A->val.p;
     a.col = A->col.p;

@@ -158,6 +158,13 @@ void launch_fill_k1(uint32_t n, uint32_t units, const uint32_t *unit_chunk,
                                                         ocol);
 }
 
+// first tile of each row (and the tile count at [n]): rpos / w
+__global__ void k_tile_starts(uint32_t n1, const uint32_t *rpos, uint32_t w, uint32_t *rt)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n1) rt[i] = rpos[i] / w;
+}
+
 __global__ void k_rowlen(uint32_t n, const uint32_t *row, uint32_t *rl)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -538,6 +545,24 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
         GS_TRY(build_rows_plan(A->rpos.as<uint32_t>(), need_rlen ? A->rlen.as<uint32_t>() : nullptr,
                                n, V, A->plan, s));
         A->plan.aligned = aligned;
+        // FP64 whole-tile layouts: the same rows over tiles for the tile kernel (windows of
+        // one 32-tile chunk).  Widths 4-16 only: at 32 a tile spans 16 lanes and 16 load
+        // steps, too few gathers in flight per lane (power-law AXC hbs 32: 846 us on the
+        // tile kernel, 516 us on the aligned row kernel; hw16 482 instead of 612 us)
+        A->tile_w = 0;
+        if (!A->tiled && !reduced && p.itype == GS_IDX_U32 &&
+            ((fmt == GS_FMT_AXT && p.mode == GS_AXT_UNC) || fmt == GS_FMT_AXC)) {
+            const uint32_t w = fmt == GS_FMT_AXC ? p.hbs : thw;
+            if (w == 4 || w == 8 || w == 16) {
+                DevBuf rt;
+                GS_TRY(rt.alloc(((size_t)n + 1) * 4));
+                k_tile_starts<<<blocks_for(n + 1), 256, 0, s>>>(n + 1, A->rpos.as<uint32_t>(), w,
+                                                                rt.as<uint32_t>());
+                GS_CHECK_LAUNCH();
+                GS_TRY(build_rows_plan(rt.as<uint32_t>(), nullptr, n, 1, A->tplan, s));
+                A->tile_w = w;
+            }
+        }
         if (p.itype == GS_IDX_U16) {
             GS_TRY(A->col.alloc_zero((size_t)A->nslots * 2, s));
             GS_TRY(build_u16_columns(col32.as<uint32_t>(), A->nslots, A->plan,

@@ -178,6 +178,10 @@ struct gs_matrix {
     // row-stream kernel configuration
     uint32_t tiled = 0;  // 1: positions map to tile slots (tileH > 1 layouts)
     gs::RowsPlan plan;
+    // FP64 layouts of whole tiles per row (UNC tileH = 1, AXC) of width 4..32: the same rows
+    // planned over tiles, for the tile kernel (launch_tiles); tile_w 0 otherwise
+    gs::RowsPlan tplan;
+    uint32_t tile_w = 0;
     double conv_ms = 0, mfp = 0, beta = 0;
 };
 
@@ -211,10 +215,12 @@ gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32
 gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &P,
                             uint16_t *d_col16, cudaStream_t s);
 RowsArgs rows_args(const RowsPlan &P);
-// Baked layouts of whole [thw values | thw x] tiles per row (UNC tileH = 1, AXC), thw in
-// {4, 8, 16, 32}: a.val = ax, the plan built over tiles (its positions are tiles, its row
-// starts the first tile of each row; windows of 32 V tiles), y FP64.
-gs_status launch_tiles_baked(const RowsArgs &a, uint32_t thw, cudaStream_t s);
+// FP64 layouts of whole tiles per row (UNC tileH = 1, AXC), thw in {4, 8, 16, 32}: baked
+// (a.val = ax: [thw values | thw x] per tile) or with value / column streams (a.val, a.col,
+// a.x; a.rbits the slot-level real bits of a padded layout, or null).  The plan is built over
+// tiles (its positions are tiles, its row starts the first tile of each row; windows of 32 V
+// tiles); y FP64.
+gs_status launch_tiles(const RowsArgs &a, uint32_t thw, bool baked, cudaStream_t s);
 gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
                       uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s);
 

@@ -609,7 +609,7 @@ static str_res run_baked(const char *name, UIN nrows, UIN nnz, const FPT *hax, U
         gs::RowsArgs a = gs::rows_args(P);
         a.val = ax.p;
         a.y = y.p;
-        return timed(name, nrows, nnz, [&]() { return gs::launch_tiles_baked(a, axw, 0); }, y,
+        return timed(name, nrows, nnz, [&]() { return gs::launch_tiles(a, axw, true, 0); }, y,
                      ref);
     }
     uint32_t V = tiled ? th : gs::kDirectV;

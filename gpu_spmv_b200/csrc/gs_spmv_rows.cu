@@ -1157,24 +1157,28 @@ __global__ void k_u16_cols(uint32_t nwin, uint32_t WS, uint32_t nslots, uint32_t
 }
 
 // ---------------------------------------------------------------------------------------
-// Baked layouts made of whole tiles per row (UNC tileH = 1: tiles of [THW values | THW x];
-// AXC: bricks of the same shape): the plan is built over tiles (a.npos = tiles, a.sbits =
-// first tile of each non-empty row), so one lane of a 32-tile chunk stands for one tile and
-// the striped segmented scan (stripe_chunk) adds tile sums into rows.  The tiles' values and
-// x are loaded cooperatively: in each of THW/2 load steps, groups of G = THW/2 lanes read 16
-// bytes of one tile's value half and the matching 16 bytes of its x half (both halves fully
-// coalesced across the warp), form two products, and sum them over the group (shuffle tree);
+// Layouts made of whole tiles per row: UNC tileH = 1 (tiles of THW slots) and AXC (bricks of
+// the same shape); baked (the reference's ax: tiles of [THW values | THW x]) or with value /
+// column streams and x gathered at run time (real slots only: the slot-level bitmap a.rbits,
+// when the layout pads).  The plan is built over tiles (a.npos = tiles, a.sbits = first tile
+// of each non-empty row), so one lane of a 32-tile chunk stands for one tile and the striped
+// segmented scan (stripe_chunk) adds tile sums into rows.  The tiles' data are loaded
+// cooperatively: in each of THW/2 load steps, groups of G = THW/2 lanes read 16 bytes of one
+// tile's values and the matching 16 bytes of its x half (baked) or 8 bytes of its columns
+// (coalesced across the warp), form two products, and sum them over the group (shuffle tree);
 // a shuffle transpose then hands tile k's sum to lane k.  Per tile: products in pairs, pairs
 // summed over a binary tree, fixed order.
-template <int THW, bool EMPTY>
-__global__ void __launch_bounds__(256) k_tiles_baked(const RowsArgs a)
+template <int THW, bool BAKED, bool EMPTY>
+__global__ void __launch_bounds__(256) k_tiles(const RowsArgs a)
 {
     constexpr int G = THW / 2;      // lanes per tile in a load step
     constexpr int TPI = 32 / G;     // tiles per load step
     constexpr int NI = G;           // load steps per 32-tile chunk
     const int lane = threadIdx.x & 31;
     double *y = static_cast<double *>(a.y);
-    const double *ax = static_cast<const double *>(a.val);
+    const double *val = static_cast<const double *>(a.val);
+    const uint32_t *col = static_cast<const uint32_t *>(a.col);
+    const double *x = static_cast<const double *>(a.x);
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const uint32_t cpwin = a.V;  // chunks per plan window
@@ -1194,10 +1198,21 @@ __global__ void __launch_bounds__(256) k_tiles_baked(const RowsArgs a)
             const uint32_t t = ch * 32u + (uint32_t)(i * TPI + gt);
             part[i] = 0.0;
             if (t < ntiles) {
-                const double *tp = ax + (size_t)t * (2 * THW) + 2 * gl;
-                const double2 v = __ldcs(reinterpret_cast<const double2 *>(tp));
-                const double2 xv = __ldcs(reinterpret_cast<const double2 *>(tp + THW));
-                part[i] = __dadd_rn(__dmul_rn(v.x, xv.x), __dmul_rn(v.y, xv.y));
+                if constexpr (BAKED) {
+                    const double *tp = val + (size_t)t * (2 * THW) + 2 * gl;
+                    const double2 v = __ldcs(reinterpret_cast<const double2 *>(tp));
+                    const double2 xv = __ldcs(reinterpret_cast<const double2 *>(tp + THW));
+                    part[i] = __dadd_rn(__dmul_rn(v.x, xv.x), __dmul_rn(v.y, xv.y));
+                } else {
+                    const uint32_t s0 = t * THW + 2u * (uint32_t)gl;  // even: one bitmap word
+                    const double2 v = __ldcs(reinterpret_cast<const double2 *>(val + s0));
+                    const uint2 c = __ldcs(reinterpret_cast<const uint2 *>(col + s0));
+                    const uint32_t rb =
+                        a.rbits ? (__ldg(a.rbits + (s0 >> 5)) >> (s0 & 31)) & 3u : 3u;
+                    const double p0 = (rb & 1u) ? __dmul_rn(v.x, __ldg(x + c.x)) : 0.0;
+                    const double p1 = (rb & 2u) ? __dmul_rn(v.y, __ldg(x + c.y)) : 0.0;
+                    part[i] = __dadd_rn(p0, p1);
+                }
             }
         }
 #pragma unroll
@@ -1244,16 +1259,16 @@ __global__ void __launch_bounds__(256) k_tiles_baked(const RowsArgs a)
     }
 }
 
-template <int THW>
-gs_status launch_tiles_baked_t(const RowsArgs &a, cudaStream_t s)
+template <int THW, bool BAKED>
+gs_status launch_tiles_t(const RowsArgs &a, cudaStream_t s)
 {
     const uint32_t nranges = (a.nwin + a.wpw - 1) / a.wpw;
     uint32_t warps = nranges;
     if (a.n_empty) warps = max(warps, min((a.n_empty + 31) / 32, 148u * 64u));
     if (warps == 0) return GS_OK;
     const uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
-    if (a.n_empty) k_tiles_baked<THW, true><<<blocks, 256, 0, s>>>(a);
-    else k_tiles_baked<THW, false><<<blocks, 256, 0, s>>>(a);
+    if (a.n_empty) k_tiles<THW, BAKED, true><<<blocks, 256, 0, s>>>(a);
+    else k_tiles<THW, BAKED, false><<<blocks, 256, 0, s>>>(a);
     GS_CHECK_LAUNCH();
     return GS_OK;
 }
@@ -1416,14 +1431,14 @@ gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtyp
                 (int)itype);
 }
 
-gs_status launch_tiles_baked(const RowsArgs &a, uint32_t thw, cudaStream_t s)
+gs_status launch_tiles(const RowsArgs &a, uint32_t thw, bool baked, cudaStream_t s)
 {
     switch (thw) {
-    case 4: return launch_tiles_baked_t<4>(a, s);
-    case 8: return launch_tiles_baked_t<8>(a, s);
-    case 16: return launch_tiles_baked_t<16>(a, s);
-    case 32: return launch_tiles_baked_t<32>(a, s);
-    default: return fail(GS_ERR_UNSUPPORTED, "tile half width %u (4, 8, 16 or 32)", thw);
+    case 4: return baked ? launch_tiles_t<4, true>(a, s) : launch_tiles_t<4, false>(a, s);
+    case 8: return baked ? launch_tiles_t<8, true>(a, s) : launch_tiles_t<8, false>(a, s);
+    case 16: return baked ? launch_tiles_t<16, true>(a, s) : launch_tiles_t<16, false>(a, s);
+    case 32: return baked ? launch_tiles_t<32, true>(a, s) : launch_tiles_t<32, false>(a, s);
+    default: return fail(GS_ERR_UNSUPPORTED, "tile width %u (4, 8, 16 or 32)", thw);
     }
 }
 
