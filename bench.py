@@ -733,7 +733,12 @@ def run_ours(args):
                   (L.GS_FLAG_STRIPED if run.get("striped") else 0) |
                   (L.GS_FLAG_ACC_F64 if run.get("acc64") else 0))
     K = args.steps
-    value = world * 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
+    nnz_all = float(nnz)  # stored elements of all ranks' blocks (each rank its own seed)
+    if dist:
+        t = torch.tensor([nnz_all], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        nnz_all = float(t[0])
+    value = 2.0 * nnz_all * K / (elapsed * 1e-3) / 1e9
     B = variant_bytes(n, nnz, kw, run)
     peak, peak_kind = measured_peak()
     achieved = B / (kern * 1e-3) / 1e9
@@ -780,15 +785,15 @@ def run_ours(args):
         pcie = pcie_bandwidth(hx, hy, dx, dy)
         step_s = max(hx.element_size() * n / (pcie["h2d_gbs_concurrent"] * 1e9),
                      hy.element_size() * n / (pcie["d2h_gbs_concurrent"] * 1e9))
-        ceiling = world * 2.0 * nnz / step_s / 1e9
-        e2e = {"value": world * 2.0 * nnz * Ke / te / 1e9, "unit": "GFLOP/s",
+        ceiling = 2.0 * nnz_all / step_s / 1e9
+        e2e = {"value": 2.0 * nnz_all * Ke / te / 1e9, "unit": "GFLOP/s",
                "pcie": pcie, "pcie_ceiling": round(ceiling, 1),
-               "frac_of_pcie_ceiling": round(2.0 * nnz * Ke / te / 1e9 / (ceiling / world), 3),
+               "frac_of_pcie_ceiling": round(2.0 * nnz_all * Ke / te / 1e9 / ceiling, 3),
                "h2d_bytes_per_step": hx.element_size() * n,
                "d2h_bytes_per_step": hy.element_size() * n, "steps": Ke,
                "path": "gs_spmv_host_stream (C ABI): per step, pinned host x -> device, "
                        "SpMV, y -> host; consecutive steps overlap on three streams",
-               "serial_value": world * 2.0 * nnz * Ke / te_serial / 1e9,
+               "serial_value": 2.0 * nnz_all * Ke / te_serial / 1e9,
                "serial_path": "gs_spmv_host, one synchronous call per step"}
 
     formats = None
