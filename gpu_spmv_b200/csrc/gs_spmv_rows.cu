@@ -240,6 +240,17 @@ __device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane
     cnt += total;
 }
 
+// Index in a baked ax ([w values | w x] per tile) of the value of slot s: shifts for the
+// power-of-two widths every layout here uses, division otherwise.
+__device__ __forceinline__ uint32_t baked_index(uint32_t s, uint32_t w)
+{
+    if ((w & (w - 1u)) == 0u) {
+        const uint32_t lg = (uint32_t)__ffs(w) - 1u;
+        return ((s >> lg) << (lg + 1u)) + (s & (w - 1u));
+    }
+    return (s / w) * 2u * w + s % w;
+}
+
 // Products of the lane's real positions, loaded from global memory (vectorised streaming
 // loads for direct layouts, one coalesced load per tile row for tiled layouts).
 template <class VT, class IT, class XT, class PT, int VM, bool TILED, bool BAKED>
@@ -263,7 +274,7 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
                     const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
                     s = t * ths + (uint32_t)k * a.thw + c;
                 }
-                const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                const uint32_t ai = baked_index(s, a.axw);
                 prod[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
             }
         }
@@ -350,7 +361,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
                     const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
                     s = t * ths + (uint32_t)k * a.thw + cc;
                 }
-                const uint32_t ai = (s / a.axw) * 2u * a.axw + s % a.axw;
+                const uint32_t ai = baked_index(s, a.axw);
                 d.v[k] = __ldcs(ax + ai);
                 d.xb[k] = __ldcs(ax + ai + a.axw);
             }
@@ -557,7 +568,7 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                                 s = t * ths + (uint32_t)k * a.thw + c;
                             }
                             const uint32_t ai = T32 ? (s >> 5) * 64u + (s & 31u)
-                                                    : (s / a.axw) * 2u * a.axw + s % a.axw;
+                                                    : baked_index(s, a.axw);
                             p[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
                         }
                     }
@@ -726,7 +737,7 @@ __global__ void __launch_bounds__(256) k_rows_striped(const RowsArgs a)
         xb = 0.0;
         if ((rm >> lane) & 1u) {
             if constexpr (BAKED) {
-                const uint32_t ai = (q / a.axw) * 2u * a.axw + q % a.axw;
+                const uint32_t ai = baked_index(q, a.axw);
                 v = __ldcs(ax + ai);
                 xb = __ldcs(ax + ai + a.axw);
             } else {
