@@ -509,6 +509,30 @@ def time_dropin(workload: str, steps: int):
             "entry_points": out}
 
 
+def gather_ceiling(A, n, nnz, kw, dx, kern_ms):
+    """The product's line requests per launch against this GPU's measured rate of random
+    8-byte reads from x (gs_gather_rate on the workload's own x): one request per x gather
+    (nnz), the value and column streams (slots x bytes / 128), and y (one request per row when
+    K1 scatters it by its permutation, else streamed).  frac = ceiling time / kernel time."""
+    import ctypes as Cc
+
+    from gpu_spmv_b200 import _lib as L
+
+    rate = Cc.c_double()
+    L.check(L.lib().gs_gather_rate(dx.data_ptr(), n, 256, Cc.byref(rate), None),
+            "gs_gather_rate")
+    slots = nnz / A.info.beta if A.info.beta > 0 else nnz
+    sv = {"f64": 8, "f32": 4, "bf16": 2}[kw.get("vtype", "f64")]
+    si = 2 if kw.get("itype") == "u16" else 4
+    k1 = kw.get("fmt") == "K1"
+    lines = nnz + slots * (sv + si) / 128.0 + (n if k1 else n * 8 / 128.0)
+    ceiling_us = lines / rate.value * 1e6
+    return {"reads_per_s_measured": rate.value, "line_requests_per_launch": lines,
+            "ceiling_us": ceiling_us, "frac": ceiling_us / (kern_ms * 1e3),
+            "note": "random 8-byte reads from x through the SM load path: the bound of an SpMV "
+                    "whose columns are uniformly random"}
+
+
 def pcie_bandwidth(hx, hy, dx, dy, reps: int = 10):
     """GB/s of pinned host -> device and device -> host copies of these buffers, alone and
     both at once (two streams), timed on the host around synchronised batches of copies."""
@@ -744,6 +768,7 @@ def run_ours(args):
     achieved = B / (kern * 1e-3) / 1e9
     tkey = f"{args.workload}/{args.variant}"
     traffic = traffic_lookup(tkey)
+    gather = gather_ceiling(A, n, nnz, kw, dx, kern) if dx.dtype == torch.float64 else None
 
     # ---- end to end through the C ABI with host buffers: H2D x, SpMV, D2H y per step
     e2e = None
@@ -842,7 +867,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "frac_of_8TBs": achieved / 8000.0, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": B, "kernel_ms": kern},
+                     "algorithmic_bytes_per_launch": B, "kernel_ms": kern,
+                     "gather_ceiling": gather},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "formats": formats,

@@ -356,6 +356,13 @@ gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const
                           const double *d_val, const double *d_x, double *d_y,
                           gs_stream stream);
 
+/* Diagnostic (no counterpart in the reference): the rate of independent random 8-byte reads
+ * from d_x[0..n) on this GPU, the ceiling of any SpMV whose x gathers hit random lines.  One
+ * timed launch after a warm-up, every SM busy, `per_thread` reads per thread (a multiple of 8;
+ * indices from a hash, all in range); *reads_per_s receives the rate.  Synchronises. */
+gs_status gs_gather_rate(const double *d_x, UIN n, UIN per_thread, double *reads_per_s,
+                         gs_stream stream);
+
 /* ---- multi-RHS products and the adjoint of y = A(v) x (K1 matrices, FP64 or FP32 values,
  * 32-bit columns).  No counterpart in the reference, which has one right-hand side and no
  * derivative.  X is row-major [ncols][k], Y row-major [nrows][k], k in {1,2,4,8,16,32},

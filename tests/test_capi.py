@@ -51,6 +51,8 @@ def test_argument_errors_need_no_gpu():
     assert lib.gs_spmv(None, None, 0, None, 0, 0, None) == L.GS_ERR_INVALID
     assert lib.gs_matrix_get_info(None, None) == L.GS_ERR_INVALID
     assert b"NULL" in lib.gs_last_error()
+    r = C.c_double()
+    assert lib.gs_gather_rate(None, 16, 8, C.byref(r), None) == L.GS_ERR_INVALID
 
 
 @pytest.mark.parametrize("case,expect", [
