@@ -56,7 +56,7 @@ def test_argument_errors_need_no_gpu():
 
 
 @pytest.mark.parametrize("case,expect", [
-    # BASELINE algorithmic bytes: nnz(s_v+s_i) + 4(n+1) + s_x n k + s_y n k
+    # algorithmic bytes of one product: nnz(s_v+s_i) + 4(n+1) + s_x n k + s_y n k
     ((262144, 262144, 1308672, 1, 8, 4, 8, 8), 20946948),
     ((4194304, 4194304, 67108864, 1, 8, 4, 8, 8), 889192452),
     ((4096000, 4096000, 109215352, 1, 8, 4, 8, 8), 1392504228),
