@@ -195,6 +195,7 @@ struct RowsArgs {
     uint32_t nslots;               // length of the value/column streams
     uint32_t n_empty;
     uint32_t aligned;              // rows start on multiples of V (aligned kernel applies)
+    uint32_t wide;                 // val and col 32-byte aligned: 32-byte stream loads
     const uint32_t *sbits, *rbits, *wcount, *ne, *empty, *colbase;
     uint32_t *status;  // device status word (bounded-wait timeouts)
     const void *val;   // value stream (or the baked ax)

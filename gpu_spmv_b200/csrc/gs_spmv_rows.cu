@@ -28,7 +28,8 @@
 //   written once with a fixed summation order: no atomics, no y zero-fill, deterministic,
 //   one launch per SpMV.
 // * Staging.  k_rows loads the value/column streams with vectorised streaming loads
-//   (direct layouts) or coalesced per-tile-row loads (tiled layouts).  k_rows_tma, for the
+//   (direct layouts: 32 bytes per lane and request when the streams are 32-byte aligned)
+//   or coalesced per-tile-row loads (tiled layouts, tileH <= 4 a window ahead).  k_rows_tma, for the
 //   tiled layouts with 32-wide tiles, streams whole tiles into a per-warp ring of shared
 //   memory stages with 1-D TMA bulk copies (cp.async.bulk, no multicast) completing on
 //   mbarriers, several tiles ahead of the warp; the L1 then serves only the x gathers,
@@ -111,6 +112,52 @@ template <> struct Load8<__nv_bfloat16> {
         }
     }
 };
+
+// 32-byte streaming loads (sm_100): a lane's 8 consecutive elements of 4 bytes in one load,
+// of 8 bytes in two, so that a warp's load instruction covers 1 KB of the stream in 8 lines
+// (16-byte loads at a 32- or 64-byte lane stride ask for each line two or four times).
+// The address must be 32-byte aligned.  Two-byte elements keep the 16-byte load, which
+// already covers a lane's 8 elements in one piece.
+template <class T> struct Load8W {
+    __device__ __forceinline__ static void run(const T *p, T (&o)[8]) { Load8<T>::run(p, o); }
+};
+template <> struct Load8W<double> {
+    __device__ __forceinline__ static void run(const double *p, double (&o)[8]) {
+        asm("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]) : "l"(p));
+        asm("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+            : "=d"(o[4]), "=d"(o[5]), "=d"(o[6]), "=d"(o[7]) : "l"(p + 4));
+    }
+};
+template <> struct Load8W<uint32_t> {
+    __device__ __forceinline__ static void run(const uint32_t *p, uint32_t (&o)[8]) {
+        asm("ld.global.cs.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(o[0]), "=r"(o[1]), "=r"(o[2]), "=r"(o[3]), "=r"(o[4]), "=r"(o[5]),
+              "=r"(o[6]), "=r"(o[7])
+            : "l"(p));
+    }
+};
+template <> struct Load8W<float> {
+    __device__ __forceinline__ static void run(const float *p, float (&o)[8]) {
+        uint32_t r[8];
+        Load8W<uint32_t>::run(reinterpret_cast<const uint32_t *>(p), r);
+#pragma unroll
+        for (int i = 0; i < 8; i++) o[i] = __uint_as_float(r[i]);
+    }
+};
+// a lane's 8 consecutive stream elements: 32-byte loads when both streams allow them
+template <class VT, class IT>
+__device__ __forceinline__ void load8_streams(bool wide, const VT *val, const IT *col,
+                                              VT (&v)[8], IT (&c)[8])
+{
+    if (wide) {
+        Load8W<VT>::run(val, v);
+        Load8W<IT>::run(col, c);
+    } else {
+        Load8<VT>::run(val, v);
+        Load8<IT>::run(col, c);
+    }
+}
 
 template <class T> __device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
 template <> __device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat16 *p) {
@@ -282,8 +329,7 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
         VT v[VM];
         IT c[VM];
         if (qb + VM <= a.nslots) {
-            Load8<VT>::run(val + qb, v);
-            Load8<IT>::run(col + qb, c);
+            load8_streams<VT, IT>(a.wide != 0u, val + qb, col + qb, v, c);
         } else {  // stream tail: element loads, never past the last slot
 #pragma unroll
             for (int k = 0; k < VM; k++) {
@@ -368,8 +414,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
         }
     } else if constexpr (!TILED) {
         if (qb + VM <= a.nslots) {
-            Load8<VT>::run(val + qb, d.v);
-            Load8<IT>::run(col + qb, d.c);
+            load8_streams<VT, IT>(a.wide != 0u, val + qb, col + qb, d.v, d.c);
         } else {  // stream tail: element loads, never past the last slot
 #pragma unroll
             for (int k = 0; k < VM; k++) {
@@ -449,7 +494,7 @@ __device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int la
 // positions per lane for direct layouts and the upper bound of th for tiled ones.  PADDED:
 // the layout has padding positions (real-bit map).  EMPTY: some rows are empty.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
-          bool BAKED, bool PADDED, bool EMPTY>
+          bool BAKED, bool PADDED, bool EMPTY, bool PF = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -471,11 +516,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
         uint32_t cnt = __ldg(a.wcount + w0);  // row starts before this range
         bool seen = (w0 == 0);                // a row start has been met in the range
         AT carry = (AT)0;
+        // PF: the next window's bits and streams are requested before this window's x
+        // gathers, so that their latency overlaps the gathers and the row sums
+        WinData<VT, IT, VM, BAKED> nxt;
+        if constexpr (PF) load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w0, lane, V, nxt);
         for (uint32_t w = w0; w < w1; w++) {
             // bits and streams are requested together (the streams do not wait for the
             // bits), then the x gathers
             WinData<VT, IT, VM, BAKED> cur;
-            load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w, lane, V, cur);
+            if constexpr (PF) {
+                cur = nxt;
+                if (w + 1 < w1) load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w + 1, lane, V, nxt);
+            } else {
+                load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w, lane, V, cur);
+            }
             const uint32_t W = w * WS;
             const WinCtl ctl = window_ctl(lane, W, V, FULLV, a.npos, cur.sraw, seen, false);
             if (ctl.skip) continue;  // all of it continues an earlier warp's row
@@ -595,8 +649,18 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                             }
                         }
                     } else {
+                        bool whole = false;
+                        if constexpr (V == 8) {
+                            // the lane's whole group (padding slots included, in bounds) in
+                            // 32-byte requests; padding products are masked below
+                            if (a.wide && qb + 8u <= a.nslots) {
+                                load8_streams<VT, IT>(true, val + qb, col + qb, v, c);
+                                whole = true;
+                            }
+                        }
 #pragma unroll
                         for (int k = 0; k < V; k++) {
+                            if (whole) break;
                             v[k] = (VT)0;
                             c[k] = 0;
                             if ((rb >> k) & 1u) {
@@ -944,8 +1008,14 @@ gs_status launch_k(const RowsArgs &a, bool padded, cudaStream_t s)
     uint32_t blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
     blocks = min(blocks, 148u * 256u);
     const bool empty = a.n_empty != 0;
+    // tiled layouts of tileH 2..4 load their streams a window ahead (COM on the power-law:
+    // th=2 575 -> 528 us, th=4 423 -> 399 us; on the 27-point stencil: th=2 860 -> 775 us,
+    // th=4 564 -> 500 us).  With tileH 5..8 (94 registers against 64) and on the direct
+    // layouts (80 against 48) the lost blocks per SM cost more than the overlap gains.
+    constexpr bool kPrefetch = TILED && VM <= 4;
 #define GS_L(P, E)                                                                          \
-    k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
+    k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E, kPrefetch>                        \
+        <<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
     if (padded) {
         if (empty) GS_L(true, true); else GS_L(true, false);
     } else {
@@ -1399,9 +1469,13 @@ RowsArgs rows_args(const RowsPlan &P)
     return a;
 }
 
-gs_status launch_rows(const RowsArgs &a, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
+gs_status launch_rows(const RowsArgs &a0, gs_dtype vtype, gs_itype itype, gs_dtype ytype,
                       uint32_t flags, bool tiled, bool baked, bool padded, cudaStream_t s)
 {
+    RowsArgs a = a0;
+    a.wide = ((reinterpret_cast<uintptr_t>(a.val) | reinterpret_cast<uintptr_t>(a.col)) & 31u)
+                 ? 0u
+                 : 1u;
     if (tiled && (a.thw == 0 || 32 % a.thw != 0))
         return fail(GS_ERR_UNSUPPORTED, "tileH>1 kernels need tileHW dividing 32 (got %u)",
                     a.thw);
