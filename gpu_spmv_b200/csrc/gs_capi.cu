@@ -139,6 +139,7 @@ gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *i)
     i->conv_ms = A->conv_ms;
     i->mfp = A->mfp;
     i->beta = A->beta;
+    i->lane_positions = (A->p.format == GS_FMT_K1 || A->tile_w) ? 0u : A->plan.V;
     return GS_OK;
 }
 
@@ -302,7 +303,9 @@ gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const
         return gs::fail(GS_ERR_INVALID, "val and col must be 16-byte aligned");
     cudaStream_t s = gs::cs(stream);
     gs::RowsPlan P;
-    GS_TRY(gs::build_rows_plan(d_row, nullptr, nrows, gs::kDirectV, P, s));
+    uint32_t V = gs::kDirectV;
+    GS_TRY(gs::direct_lane_positions(d_row, d_col, nrows, nnz, &V, s));
+    GS_TRY(gs::build_rows_plan(d_row, nullptr, nrows, V, P, s));
     gs::RowsArgs a = gs::rows_args(P);
     a.val = d_val;
     a.col = d_col;

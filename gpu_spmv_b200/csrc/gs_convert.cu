@@ -530,6 +530,8 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
         // width V is chosen to divide that alignment so the aligned kernel applies.
         uint32_t V = kDirectV;
         bool aligned = false;
+        if (!reduced && !A->tiled && !need_rlen)  // FP64 CSR and COM tileH = 1
+            GS_TRY(direct_lane_positions(d_row, d_col, n, nnz, &V, s));
         if (A->tiled) {
             V = th;
             aligned = fmt == GS_FMT_AXT && p.mode == GS_AXT_UNC &&

@@ -205,6 +205,14 @@ struct RowsArgs {
 };
 // Positions per lane of the direct (tileH = 1) layouts.
 constexpr uint32_t kDirectV = 8;
+// Positions per lane of an FP64 direct layout with x gathered at run time (CSR, COM
+// tileH = 1), from the CSR row pointers and columns: 4 when rows average fewer than 8
+// elements or fewer than a quarter of a sample of in-row column steps stay within 16
+// columns (the x gathers are random: 4 positions hold 40 registers, 6 blocks per SM, and a
+// lane's 4 values and 4 columns are one 32-byte and one 16-byte request), else 8 (streams
+// with local columns: more bytes in flight per warp).
+gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
+                                uint64_t nnz, uint32_t *V, cudaStream_t s);
 // Positions per lane for a layout whose rows start on multiples of `align` positions
 // (0: no alignment): returns the V that makes the aligned kernel apply, or kDirectV.
 uint32_t aligned_lane_positions(uint32_t align, bool *aligned);

@@ -502,8 +502,10 @@ str_res test_gcsr(const UIN cudaBlockSize, const str_matCSR m, const FPT *vec, c
     (void)cudaBlockSize;
     DevBuf row, col, val, x, y;
     gs::RowsPlan P;
+    uint32_t V = gs::kDirectV;
     if (upload_csr(m, row, col, val) || h2d(x, vec, m.nrows) || y.alloc((size_t)m.nrows * 8) ||
-        gs::build_rows_plan(row.as<UIN>(), nullptr, m.nrows, gs::kDirectV, P, 0))
+        gs::direct_lane_positions(row.as<UIN>(), col.as<UIN>(), m.nrows, m.nnz, &V, 0) ||
+        gs::build_rows_plan(row.as<UIN>(), nullptr, m.nrows, V, P, 0))
         return error_res("gcsr", gs_last_error());
     gs::RowsArgs a = gs::rows_args(P);
     a.val = val.p;

@@ -159,6 +159,34 @@ __device__ __forceinline__ void load8_streams(bool wide, const VT *val, const IT
     }
 }
 
+// a lane's VM consecutive stream elements from a VM-aligned index: 8 as above; 4 FP64 values
+// (32 bytes: one request when wide) with 4 32-bit columns (one 16-byte load)
+template <class VT, class IT, int VM>
+__device__ __forceinline__ void load_streams(bool wide, const VT *val, const IT *col,
+                                             VT (&v)[VM], IT (&c)[VM])
+{
+    if constexpr (VM == 8) {
+        load8_streams<VT, IT>(wide, val, col, v, c);
+    } else if constexpr (VM == 4 && sizeof(VT) == 8 && sizeof(IT) == 4) {
+        if (wide) {
+            asm("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+                : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(val));
+        } else {
+            const double2 a = __ldcs(reinterpret_cast<const double2 *>(val));
+            const double2 b = __ldcs(reinterpret_cast<const double2 *>(val) + 1);
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        }
+        const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(col));
+        c[0] = q.x; c[1] = q.y; c[2] = q.z; c[3] = q.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < VM; k++) {
+            v[k] = __ldcs(val + k);
+            c[k] = __ldcs(col + k);
+        }
+    }
+}
+
 template <class T> __device__ __forceinline__ T ld_stream(const T *p) { return __ldcs(p); }
 template <> __device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat16 *p) {
     return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short *>(p)));
@@ -329,7 +357,7 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
         VT v[VM];
         IT c[VM];
         if (qb + VM <= a.nslots) {
-            load8_streams<VT, IT>(a.wide != 0u, val + qb, col + qb, v, c);
+            load_streams<VT, IT, VM>(a.wide != 0u, val + qb, col + qb, v, c);
         } else {  // stream tail: element loads, never past the last slot
 #pragma unroll
             for (int k = 0; k < VM; k++) {
@@ -414,7 +442,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
         }
     } else if constexpr (!TILED) {
         if (qb + VM <= a.nslots) {
-            load8_streams<VT, IT>(a.wide != 0u, val + qb, col + qb, d.v, d.c);
+            load_streams<VT, IT, VM>(a.wide != 0u, val + qb, col + qb, d.v, d.c);
         } else {  // stream tail: element loads, never past the last slot
 #pragma unroll
             for (int k = 0; k < VM; k++) {
@@ -1160,8 +1188,14 @@ gs_status launch_shape(const RowsArgs &a, bool tiled, bool padded, uint32_t flag
             default: break;
             }
         }
-        if (a.V != kDirectV) return fail(GS_ERR_INVALID, "plan built for another shape");
+        // FP64 direct layouts with run-time x: 4 or 8 positions per lane
+        // (direct_lane_positions); the striped kernel takes either plan
+        if (a.V != kDirectV && (BAKED || a.V != 4))
+            return fail(GS_ERR_INVALID, "plan built for another shape");
         if (striped) return launch_striped<VT, IT, XT, PT, AT, YT, BAKED>(a, padded, s);
+        if constexpr (!BAKED) {
+            if (a.V == 4) return launch_k<VT, IT, XT, PT, AT, YT, 4, false, BAKED>(a, padded, s);
+        }
         return launch_k<VT, IT, XT, PT, AT, YT, 8, false, BAKED>(a, padded, s);
     }
 }
@@ -1186,6 +1220,31 @@ __global__ void k_set_real(uint32_t n, const uint32_t *rpos, const uint32_t *rle
         const uint32_t m = (cnt == 32 ? 0xffffffffu : ((1u << cnt) - 1u)) << b;
         atomicOr(rbits + w, m);
         p += cnt;
+    }
+}
+
+// Column locality of a CSR matrix, sampled: rows r = t * stride (t < samples), the first
+// 33 elements of each; cnt[0] += in-row steps, cnt[1] += steps |col[e] - col[e-1]| < 16 (the
+// next column within one 128-byte line of FP64 x).
+__global__ void k_col_steps(const uint32_t *row, const uint32_t *col, uint32_t stride,
+                            uint32_t samples, unsigned long long *cnt)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t steps = 0, near = 0;
+    if (t < samples) {
+        const uint32_t r = t * stride;
+        const uint32_t b = row[r], e = min(row[r + 1], b + 33u);
+        for (uint32_t i = b + 1; i < e; i++) {
+            const uint32_t c0 = col[i - 1], c1 = col[i];
+            steps++;
+            near += (c1 > c0 ? c1 - c0 : c0 - c1) < 16u ? 1u : 0u;
+        }
+    }
+    steps = __reduce_add_sync(0xffffffffu, steps);
+    near = __reduce_add_sync(0xffffffffu, near);
+    if ((threadIdx.x & 31) == 0 && steps) {
+        atomicAdd(cnt, (unsigned long long)steps);
+        atomicAdd(cnt + 1, (unsigned long long)near);
     }
 }
 
@@ -1355,6 +1414,31 @@ gs_status launch_tiles_t(const RowsArgs &a, cudaStream_t s)
 }
 
 }  // namespace
+
+gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
+                                uint64_t nnz, uint32_t *V, cudaStream_t s)
+{
+    *V = kDirectV;
+    if (n == 0 || nnz == 0) return GS_OK;
+    if ((double)nnz / (double)n < 8.0) {  // short rows: more warps beat longer lanes
+        *V = 4;
+        return GS_OK;
+    }
+    const uint32_t samples = n < 65536u ? n : 65536u;
+    const uint32_t stride = n / samples;
+    DevBuf cnt;
+    GS_TRY(cnt.alloc_zero(16, s));
+    k_col_steps<<<(samples + 255) / 256, 256, 0, s>>>(d_row, d_col, stride, samples,
+                                                      cnt.as<unsigned long long>());
+    GS_CHECK_LAUNCH();
+    unsigned long long h[2] = {0, 0};
+    GS_CUDA(cudaMemcpyAsync(h, cnt.p, 16, cudaMemcpyDeviceToHost, s));
+    GS_CUDA(cudaStreamSynchronize(s));
+    // fewer than a quarter of the steps stay within a line: the x gathers are (close to)
+    // random and set the pace
+    if (h[1] * 4 < h[0]) *V = 4;
+    return GS_OK;
+}
 
 gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
                           uint32_t V, RowsPlan &P, cudaStream_t s)

@@ -296,6 +296,8 @@ typedef struct {
     double conv_ms; /* device time of the conversion */
     double mfp;     /* memory footprint as the reference counts it (bytes) */
     double beta;    /* occupancy nnz / stored slots */
+    UIN lane_positions; /* consecutive positions per lane of the row-stream kernel (0: the
+                         * matrix runs on the K1 or the tile kernel) */
 } gs_matrix_info;
 gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *info);
 

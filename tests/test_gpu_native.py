@@ -215,3 +215,41 @@ def test_create_from_host_arrays(port):
     A = E.Matrix(row, col, val, ncols=n, fmt="AXT", mode="UNC", tileH=4, tileHW=32)
     assert torch.equal(y, A.spmv(x))
     L.lib().gs_matrix_destroy(h)
+
+
+def _lane_case(kind):
+    from gpu_spmv_b200 import matgen
+
+    if kind == "random":  # 10-40 uniformly random columns per row: gather-bound
+        rng = np.random.default_rng(11)
+        from mats import csr_from_lengths
+        return csr_from_lengths(rng.integers(10, 41, 6000), 6000, rng)
+    if kind == "banded":  # 20-40 columns in a band of 129: local columns
+        return matgen.banded(20000, 64, 20, 40, seed=12)
+    return matgen.laplacian2d(96)  # 5 per row
+
+
+@pytest.mark.parametrize("kind,expect", [("random", 4), ("banded", 8), ("short", 4)])
+@pytest.mark.parametrize("fmt", [dict(fmt="CSR"), dict(fmt="AXT", mode="COM", tileH=1, tileHW=32)],
+                         ids=["csr", "com1"])
+def test_lane_positions_choice(port, kind, expect, fmt):
+    """FP64 CSR / COM tileH=1 products take 4 positions per lane when their x gathers are
+    random or their rows short, 8 when rows of local columns stream; both meet the bound,
+    and so does the device-array CSR entry point, which makes the same choice per call."""
+    from gpu_spmv_b200 import engine as E
+
+    row, col, val = _lane_case(kind)
+    n = len(row) - 1
+    A = E.Matrix(row, col, val, ncols=n, **fmt)
+    assert A._info().lane_positions == expect
+    x = np.random.default_rng(3).uniform(-1, 1, n)
+    y_ref = port.csr_spmv(row, col, val, x)
+    _, mag = port.csr_truth(row, col, val, x)
+    assert within_bound(A.spmv(torch.from_numpy(x).cuda()).cpu().numpy(), y_ref, mag)
+    assert within_bound(A.spmv(torch.from_numpy(x).cuda(), striped=True).cpu().numpy(), y_ref,
+                        mag)
+    A.close()
+    dev = torch.device("cuda")
+    y = E.csr_spmv_f64(E.to_device_u32(row, dev), E.to_device_u32(col, dev),
+                       torch.from_numpy(val).cuda(), torch.from_numpy(x).cuda())
+    assert within_bound(y.cpu().numpy(), y_ref, mag)
