@@ -425,6 +425,17 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
     const uint32_t ths = a.th * a.thw;
     if constexpr (BAKED) {
         const double *ax = static_cast<const double *>(a.val);
+        if constexpr (!TILED && VM == 8) {
+            // 8 dividing the tile width, a lane's 8 slots lie in one tile: its values and its
+            // x are two runs of 8 consecutive doubles (two 32-byte loads each; slots past
+            // npos are the last tile's zero fill, masked by the caller)
+            if (a.wide && (a.axw & 7u) == 0u && qb < a.npos) {
+                const uint32_t ai = baked_index(qb, a.axw);
+                Load8W<double>::run(ax + ai, d.v);
+                Load8W<double>::run(ax + ai + a.axw, d.xb);
+                return;
+            }
+        }
 #pragma unroll
         for (int k = 0; k < VM; k++) {
             d.v[k] = 0.0;

@@ -253,3 +253,43 @@ def test_lane_positions_choice(port, kind, expect, fmt):
     y = E.csr_spmv_f64(E.to_device_u32(row, dev), E.to_device_u32(col, dev),
                        torch.from_numpy(val).cuda(), torch.from_numpy(x).cuda())
     assert within_bound(y.cpu().numpy(), y_ref, mag)
+
+
+@pytest.mark.parametrize("fmt", [dict(fmt="CSR"), dict(fmt="CSR", vtype="f32"),
+                                 dict(fmt="AXT", mode="COM", tileH=1, tileHW=32),
+                                 dict(fmt="AXT", mode="COM", tileH=4, tileHW=32),
+                                 dict(fmt="AXT", mode="COM", tileH=6, tileHW=32),
+                                 dict(fmt="AXT", mode="UNC", tileH=6, tileHW=32)],
+                         ids=["csr", "csr-f32", "com1", "com4", "com6", "unc6"])
+def test_rows_across_warp_ranges(port, fmt):
+    """Rows much longer than a warp's range of windows (up to 70,000 elements, next to empty
+    and one-element rows; the warp where a row starts sums it past its range end): the bound
+    holds and repeated products are bit-identical."""
+    from gpu_spmv_b200 import engine as E
+    from mats import csr_from_lengths
+
+    rng = np.random.default_rng(21)
+    lens = rng.integers(0, 9, 4000)
+    for i, L in ((0, 70000), (1, 1), (2, 4095), (3, 0), (4, 33000), (900, 1024), (901, 2048),
+                 (2000, 50000), (3999, 12345)):
+        lens[i] = L
+    row, col, val = csr_from_lengths(lens, 200000, rng)
+    A = E.Matrix(row, col, val, ncols=200000, **fmt)
+    f32 = fmt.get("vtype") == "f32"
+    x = rng.uniform(-1, 1, 200000)
+    xd = torch.from_numpy(x).cuda()
+    if f32:
+        xd = xd.float()
+    y1 = A.spmv(xd)
+    y2 = A.spmv(xd)
+    assert torch.equal(y1, y2)
+    y = y1.double().cpu().numpy()
+    exact, mag = port.csr_truth(row, col, val, x.astype(np.float32).astype(np.float64) if f32 else x)
+    if f32:
+        lensf = np.diff(row).astype(np.float64)
+        vals32 = val.astype(np.float32).astype(np.float64)
+        e32, m32 = port.csr_truth(row, col, vals32, x.astype(np.float32).astype(np.float64))
+        assert np.all(np.abs(y - e32) <= 2.0 ** -24 * (3 + lensf) * m32 + 1e-30)
+    else:
+        assert within_bound(y, port.csr_spmv(row, col, val, x), mag)
+    A.close()
