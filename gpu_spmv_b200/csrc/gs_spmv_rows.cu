@@ -1462,9 +1462,11 @@ gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32
     P.npos = npos;
     const uint64_t WS = 32ull * V;
     P.nwin = (uint32_t)(((uint64_t)npos + WS - 1) / WS);
-    // windows per warp range of the LDG kernel: ~1024 positions, fewer when the matrix is
-    // too small to give every SM enough warps
-    uint32_t wpw = (uint32_t)((1024 + WS - 1) / WS);
+    // windows per warp range of the LDG kernels: ~2048 positions at 8 per lane (27-point
+    // stencil against ~1024: CSR 330 -> 318 us, COM th=8 547 -> 471, UNC th=8 448 -> 408;
+    // power-law: COM th=8 437 -> 409, UNC th=8 364 -> 343), ~1024 otherwise; fewer when the
+    // matrix is too small to give every SM enough warps
+    uint32_t wpw = (uint32_t)(((V == 8 ? 2048u : 1024u) + WS - 1) / WS);
     while (wpw > 1 && (uint64_t)P.nwin / wpw < 148ull * 48ull) wpw >>= 1;
     P.wpw = wpw;
     const size_t words = (size_t)P.nwin * V + 2;
