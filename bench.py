@@ -113,8 +113,12 @@ DEFAULT_VARIANT = "k1"
 COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc")
 
 
-def make_matrix(workload: str, rank: int):
-    from gpu_spmv_b200 import matgen
+def make_matrix(workload: str, rank: int, matgen=None):
+    """The workload's CSR arrays and x.  `matgen` is the generator module: the engine's
+    (gpu_spmv_b200.matgen) for this engine's arm, the same source built apart from the engine
+    (oracle.workload) for the reference arm; both give the same bytes for a seed."""
+    if matgen is None:
+        from gpu_spmv_b200 import matgen
 
     w = WORKLOADS[workload]
     if workload == "powerlaw":
@@ -133,6 +137,28 @@ def make_matrix(workload: str, rank: int):
     else:
         raise KeyError(workload)
     return row, col, val, x
+
+
+def loaded_repo_libraries() -> list:
+    """Shared libraries of this repository mapped into this process (from /proc/self/maps)."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and os.path.realpath(path).startswith(os.path.realpath(ROOT)):
+                    out.add(os.path.relpath(os.path.realpath(path), os.path.realpath(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def workload_config(workload: str, n: int, nnz: int, world: int) -> dict:
+    """The `config` object of the JSON line, the same for both arms on one workload."""
+    return {"workload": WORKLOADS[workload]["desc"], "nrows": n, "nnz": nnz,
+            "l2": "value/column streams > 126 MB L2 each step; no flush",
+            "per_rank": ("independent partition of the same size (block-diagonal)"
+                         if world > 1 else "one matrix")}
 
 
 def measured_peak():
@@ -270,22 +296,26 @@ def cpu_details(row, col, val, x, block_rows: int = 1 << 18, reps: int = 5):
 
 
 def error_vs_fp64(row, col, val, x, y) -> float:
-    """max_i |y_i - y64_i| / (|A||x|)_i of a reduced-precision product y against the FP64
-    product (the engine's K1 FP64 path, itself within 1e-13 of the reference's CPU loop)."""
+    """max_i |y_i - y64_i| / (|A||x|)_i of a product y against an FP64 product computed
+    outside this engine (torch's sparse CSR product, cuSPARSE, on the same device), with
+    (|A||x|)_i from the same library on |A| and |x|."""
     import torch
 
-    from gpu_spmv_b200 import engine as E
-
     n = len(row) - 1
-    dx = torch.from_numpy(x).cuda()
-    A = E.Matrix(row, col, val, ncols=n, fmt="K1")
-    y64 = A.spmv(dx)
-    A.close()
-    M = E.Matrix(row, col, np.abs(val), ncols=n, fmt="K1")
-    mag = M.spmv(dx.abs())
-    M.close()
+    dev = y.device
+    crow = torch.from_numpy(row.astype(np.int64)).to(dev)
+    cols = torch.from_numpy(col.astype(np.int64)).to(dev)
+    v = torch.from_numpy(val).to(dev)
+    dx = torch.from_numpy(x).to(dev)
+    A = torch.sparse_csr_tensor(crow, cols, v, size=(n, len(x)))
+    y64 = (A @ dx[:, None])[:, 0]
+    Aa = torch.sparse_csr_tensor(crow, cols, v.abs(), size=(n, len(x)))
+    mag = (Aa @ dx.abs()[:, None])[:, 0]
     r = (y.double() - y64).abs() / mag.clamp_min(1e-300)
-    return float(r.max())
+    out = float(r.max())
+    del A, Aa, crow, cols, v
+    torch.cuda.empty_cache()
+    return out
 
 
 def _time_us(fn, steps: int, warm: int = 5) -> float:
@@ -328,7 +358,7 @@ def time_mixed(steps: int):
         y = torch.empty(n, dtype=torch.float64 if (not kw or acc) else torch.float32,
                         device="cuda")
         us = _time_us(lambda: A.spmv(dx, y, acc64=acc), steps)
-        err = 0.0 if not kw else error_vs_fp64(row, col, val, x, y)
+        err = error_vs_fp64(row, col, val, x, y)
         out[name] = {"us": round(us, 2), "gflops": round(2.0 * nnz / us / 1e3, 1),
                      "error_vs_fp64": err}
         A.close()
@@ -408,15 +438,13 @@ def time_batched(steps: int, count: int = 256):
     from gpu_spmv_b200 import engine as E
     from gpu_spmv_b200 import matgen
 
-    rng = np.random.default_rng(3)
     nm = count
-    nrows = np.exp(rng.uniform(np.log(1000), np.log(200000), nm)).astype(np.int64)
-    hbw = rng.integers(16, 257, nm)
-    ks = [int(k) for k in rng.integers(1, 33, nm)]
-    mats, plain_us, nnz_tot = [], 0.0, 0
-    for i in range(nm):
-        row, col, val = matgen.banded(int(nrows[i]), int(hbw[i]), 5, 60, seed=3000 + i)
+    work = matgen.banded_batch(nm, seed=3)
+    ks = [w[3] for w in work]
+    mats, plain_us, nnz_tot, nrows_tot = [], 0.0, 0, 0
+    for i, (row, col, val, _) in enumerate(work):
         n = len(row) - 1
+        nrows_tot += n
         nnz_tot += len(col)
         mats.append(E.Matrix(row, col, val, ncols=n, fmt="K1", vtype="f32"))
         A64 = E.Matrix(row, col, val, ncols=n, fmt="K1")
@@ -425,8 +453,8 @@ def time_batched(steps: int, count: int = 256):
         plain_us += ks[i] * _time_us(lambda: A64.spmv(x, y), 5, warm=2)
         A64.close()
     B = E.Batch(mats, ks)
-    g = torch.Generator().manual_seed(3)
-    B.make_operands([torch.randn(A.ncols, k, generator=g) for A, k in zip(mats, ks)])
+    B.make_operands([matgen.batch_rhs(i, A.ncols, k, seed=3) for i, (A, k) in
+                     enumerate(zip(mats, ks))])
     tune = autotune.tune(B, reps=5)
     us = _time_us(lambda: B.run(graph=True), steps, warm=3)
     us_default = None
@@ -438,9 +466,24 @@ def time_batched(steps: int, count: int = 256):
     B.set_paths(["k1"] * nm)  # every matrix on K1 units (gathers through L1 / L2)
     us_k1 = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
     B.set_paths(["auto"] * nm)
+    # error of every matrix's FP32 result against the FP64 product of the same FP32 values and
+    # right-hand sides (torch's sparse CSR product, outside this engine), per row over
+    # (|A||X|)_i: the largest over all matrices and columns
+    B.run(graph=True)
+    torch.cuda.synchronize()
+    err = 0.0
+    for (row, col, val, k), Y, X in zip(work, B.results(), B.X):
+        n = len(row) - 1
+        crow = torch.from_numpy(row.astype(np.int64)).cuda()
+        cols = torch.from_numpy(col.astype(np.int64)).cuda()
+        v = torch.from_numpy(val.astype(np.float32).astype(np.float64)).cuda()
+        X64 = X[:, :k].double()
+        y64 = torch.sparse_csr_tensor(crow, cols, v, size=(n, n)) @ X64
+        mag = torch.sparse_csr_tensor(crow, cols, v.abs(), size=(n, n)) @ X64.abs()
+        err = max(err, float(((Y.double() - y64).abs() / mag.clamp_min(1e-300)).max()))
     flops = B.flops
     out = {"workload": "%d banded FP32 matrices, %d rows, %d nnz, 1-32 RHS (sum %d), seed 3"
-                       % (nm, int(nrows.sum()), nnz_tot, sum(ks)),
+                       % (nm, nrows_tot, nnz_tot, sum(ks)),
            "us_per_run": round(us, 1), "gflops": round(flops / us / 1e3, 1),
            "us_per_run_untuned": round(us_default, 1),
            "work_items": B.nitems,
@@ -449,6 +492,9 @@ def time_batched(steps: int, count: int = 256):
            "plain_fp64_us": round(plain_us, 1),
            "plain_fp64_gflops": round(flops / plain_us / 1e3, 1),
            "speedup_vs_plain_fp64": round(plain_us / us, 2),
+           "error_vs_fp64": err,
+           "error_note": "max over all matrices, rows and columns of |Y - Y64| / (|A||X|)_i, "
+                         "Y64 = torch sparse CSR FP64 product of the same FP32 numbers",
            "autotune": {k: int(v) for k, v in tune["choices"].items()},
            "autotune_ms": {k: round(v, 3) for k, v in tune["timings"].items()}}
     B.close()
@@ -509,18 +555,83 @@ def time_dropin(workload: str, steps: int):
             "entry_points": out}
 
 
+PROBE_SO = os.path.join(ROOT, "gpu_spmv_b200", "lib", "libgs_bench_probe.so")
+_probe = None
+
+
+def probe_lib():
+    """The benchmark's measurement helpers (gs_bench_probe.cu), not part of the engine."""
+    global _probe
+    if _probe is None:
+        import ctypes as Cc
+
+        lib = Cc.CDLL(PROBE_SO)
+        lib.gsp_last_error.restype = Cc.c_char_p
+        lib.gsp_gather_rate.restype = Cc.c_int
+        lib.gsp_gather_rate.argtypes = [Cc.c_void_p, Cc.c_uint32, Cc.c_uint32,
+                                        Cc.POINTER(Cc.c_double), Cc.c_void_p]
+        lib.gsp_gather4_rate.restype = Cc.c_int
+        lib.gsp_gather4_rate.argtypes = [Cc.c_void_p, Cc.c_uint32, Cc.c_uint32, Cc.c_uint32,
+                                         Cc.c_uint32, Cc.c_uint32, Cc.POINTER(Cc.c_double),
+                                         Cc.POINTER(Cc.c_uint32), Cc.c_void_p]
+        _probe = lib
+    return _probe
+
+
+def gather_rate(dx, n) -> float:
+    """Random 8-byte reads per second from dx[0..n) through the SM load path."""
+    import ctypes as Cc
+
+    rate = Cc.c_double()
+    lib = probe_lib()
+    if lib.gsp_gather_rate(dx.data_ptr(), n, 256, Cc.byref(rate), None):
+        raise RuntimeError(f"gsp_gather_rate: {lib.gsp_last_error().decode()}")
+    return rate.value
+
+
+def gather4_rates(dx, n, per_lane: int = 256):
+    """Random reads per second from dx when issued as TMA tile::gather4 loads (four 16-byte
+    rows per instruction into shared memory), alone and beside load-path gathers in the same
+    blocks: {config: reads/s}.  Raises if a bounded wait gave up."""
+    import ctypes as Cc
+
+    lib = probe_lib()
+    out = {}
+    n2 = n & ~1
+    for warps, lsu, bps in ((4, 0, 2), (8, 0, 2), (8, 0, 3), (8, 4, 2), (8, 2, 2), (8, 8, 2)):
+        rate, to = Cc.c_double(), Cc.c_uint32()
+        if lib.gsp_gather4_rate(dx.data_ptr(), n2, per_lane, warps, lsu, bps, Cc.byref(rate),
+                                Cc.byref(to), None):
+            raise RuntimeError(f"gsp_gather4_rate: {lib.gsp_last_error().decode()}")
+        if to.value:
+            raise RuntimeError("gsp_gather4_rate: a bounded wait gave up")
+        out[f"{bps}x{warps}warps_{lsu}lsu"] = rate.value
+    return out
+
+
+def time_gathers(workload: str):
+    """Random-read rates from the workload's x (n doubles): the load path alone, and TMA
+    tile::gather4 loads alone and beside load-path gathers in the same blocks."""
+    import torch
+
+    from gpu_spmv_b200 import matgen
+
+    n = {"powerlaw": 4194304, "powerlaw-small": 1048576, "stencil27": 4096000}.get(workload,
+                                                                                    4194304)
+    dx = torch.from_numpy(matgen.vector(n, "uniform", -1.0, 1.0, seed=1001)).cuda()
+    out = {"n": n, "bytes": 8 * n, "load_path_reads_per_s": gather_rate(dx, n)}
+    out["tma_gather4_reads_per_s"] = gather4_rates(dx, n)
+    return out
+
+
 def gather_ceiling(A, n, nnz, kw, dx, kern_ms):
     """The product's line requests per launch against this GPU's measured rate of random
-    8-byte reads from x (gs_gather_rate on the workload's own x): one request per x gather
+    8-byte reads from x (gsp_gather_rate on the workload's own x): one request per x gather
     (nnz), the value and column streams (slots x bytes / 128), and y (one request per row when
     K1 scatters it by its permutation, else streamed).  frac = ceiling time / kernel time."""
     import ctypes as Cc
 
-    from gpu_spmv_b200 import _lib as L
-
-    rate = Cc.c_double()
-    L.check(L.lib().gs_gather_rate(dx.data_ptr(), n, 256, Cc.byref(rate), None),
-            "gs_gather_rate")
+    rate = Cc.c_double(gather_rate(dx, n))
     slots = nnz / A.info.beta if A.info.beta > 0 else nnz
     sv = {"f64": 8, "f32": 4, "bf16": 2}[kw.get("vtype", "f64")]
     si = 2 if kw.get("itype") == "u16" else 4
@@ -569,7 +680,8 @@ def pcie_bandwidth(hx, hy, dx, dy, reps: int = 10):
 
 def time_formats(row, col, val, x, steps: int):
     """µs per product of the other formats and of cuSPARSE CSR on the same matrix and x
-    (per-launch CUDA events, mean over `steps` launches after warm-up)."""
+    (per-launch CUDA events, mean over `steps` launches after warm-up), and each format's
+    max_i |y - y64|_i / (|A||x|)_i against torch's FP64 sparse CSR product."""
     import torch
 
     from gpu_spmv_b200 import _lib as L
@@ -579,7 +691,7 @@ def time_formats(row, col, val, x, steps: int):
     n = len(row) - 1
     dx = torch.from_numpy(x).cuda()
     dy = torch.empty(n, dtype=torch.float64, device="cuda")
-    out = {}
+    out, errs = {}, {}
     for vname in COMPARE:
         kw = dict(VARIANTS[vname])
         A = E.Matrix(row, col, val, ncols=n, **kw)
@@ -595,6 +707,7 @@ def time_formats(row, col, val, x, steps: int):
         torch.cuda.synchronize()
         out[vname] = round(1e3 * sum(a.elapsed_time(b) for a, b in ts) / steps, 2)
         A.close()
+        errs[vname] = error_vs_fp64(row, col, val, x, dy)
     # cuSPARSE generic CSR SpMV through the drop-in test_gcucsr (per-launch events)
     h = R.csr_struct(row, col, val)
     ref = dy.cpu().numpy()
@@ -606,6 +719,7 @@ def time_formats(row, col, val, x, steps: int):
         out["cusparse-csr"] = round(r.et * 1e6, 2) if r.name == b"gcucsr" else None
     finally:
         L.lib().gs_set_num_ite(old)
+    out["error_vs_fp64"] = errs
     return out
 
 
@@ -621,7 +735,9 @@ def run_reference(args):
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build missing: {e}"}))
         return 0
-    row, col, val, x = make_matrix(args.workload, 0)
+    from oracle import workload as oracle_workload
+
+    row, col, val, x = make_matrix(args.workload, 0, oracle_workload)
     from oracle.oracle import Ref
 
     R = Ref()
@@ -659,13 +775,16 @@ def run_reference(args):
             "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOADS[args.workload]["desc"],
-                       "path": "reference ncsr (cudaSpmv.cu:451-466, OpenMP, compiled "
-                               "unchanged)", "threads": threads},
+            "config": workload_config(args.workload, n, nnz, args.gpus),
+            "path": {"impl": "reference ncsr (cudaSpmv.cu:451-466, OpenMP, compiled "
+                             "unchanged into oracle/_ref)", "threads": threads,
+                     "inputs": "oracle/_build/libgs_workload.so (the benchmark generator "
+                               "built apart from the engine)"},
             "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "loaded_libraries": loaded_repo_libraries()}
     print(json.dumps(line))
     return 0
 
@@ -743,7 +862,7 @@ def run_ours(args):
         if args.sweep and rank == 0:
             gf = 2.0 * nnz * K / (elapsed * 1e-3) / 1e9
             B = variant_bytes(n, nnz, kw, run)
-            err = error_vs_fp64(row, col, val, x, dy) if not f64 else 0.0
+            err = error_vs_fp64(row, col, val, x, dy)
             print(f"[sweep] {vname:18s} {elapsed / K * 1e3:9.1f} us/step  {gf:8.1f} GFLOP/s  "
                   f"{B / (kern * 1e-3) / 1e9:8.1f} GB/s alg  beta={A.info.beta:.3f} "
                   f"conv={A.info.conv_ms:.1f} ms  err={err:.2e}", file=sys.stderr, flush=True)
@@ -858,12 +977,9 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": elapsed / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": kw.get("vtype", "f64"),
         "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload]["desc"],
-                   "format": args.variant,
-                   "error_vs_fp64": (None if kw.get("vtype", "f64") == "f64" else
-                                     error_vs_fp64(row, col, val, x, dy)), "nrows": n, "nnz": nnz, "beta": info.beta,
-                   "l2": "value/column streams > 126 MB L2 each step; no flush",
-                   "per_rank": "independent partition of the same size (block-diagonal)"},
+        "config": workload_config(args.workload, n, nnz, world),
+        "path": {"format": args.variant, "beta": info.beta,
+                 "error_vs_fp64": error_vs_fp64(row, col, val, x, dy)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "frac_of_8TBs": achieved / 8000.0, "traffic": traffic,
@@ -898,7 +1014,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--only", choices=["mixed", "adjoint", "batched", "batched-small", "dropin"],
+    ap.add_argument("--only", choices=["mixed", "adjoint", "batched", "batched-small", "dropin",
+                                       "gathers"],
                     help="run one section alone and print its object (dropin: the reference's "
                          "converters and test_* entry points, through this library, on --workload)")
     ap.add_argument("--format-steps", type=int, default=200)
@@ -916,7 +1033,8 @@ def main():
               "adjoint": lambda: time_adjoint(args.steps),
               "batched": lambda: time_batched(args.steps),
               "batched-small": lambda: time_batched(args.steps, count=32),
-              "dropin": lambda: time_dropin(args.workload, args.steps)}[args.only]
+              "dropin": lambda: time_dropin(args.workload, args.steps),
+              "gathers": lambda: time_gathers(args.workload)}[args.only]
         print(json.dumps({args.only: fn()}))
         return 0
     return run_ours(args)

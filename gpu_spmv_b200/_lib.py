@@ -177,6 +177,7 @@ SIGNATURES = {
                                     _vp, _vp, _vp, C.c_int, _vp]),
     "gs_matrix_destroy": (_st, [_vp]),
     "gs_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
+    "gs_dropin_last_y": (UIN, [FPTp, UIN]),
     "gs_algorithmic_bytes": (C.c_double, [UIN, UIN, UIN, UIN, UIN, UIN, UIN, UIN]),
     "gs_spmv": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, UIN, _vp]),
     "gs_spmv_host": (_st, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_int, UIN, _vp]),
@@ -190,7 +191,6 @@ SIGNATURES = {
     "gs_matrix_value_slots": (_st, [_vp, C.POINTER(UIN)]),
     "gs_matrix_convert_values": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, _vp]),
     "gs_spmm_adjoint": (_st, [_vp, _vp, _vp, _vp, _vp, C.c_int, UIN, C.c_int, C.c_int, _vp]),
-    "gs_gather_rate": (_st, [_vp, UIN, UIN, C.POINTER(C.c_double), _vp]),
     "gs_batch_create": (_st, [C.POINTER(_vp), UIN, C.POINTER(_vp), C.POINTER(UIN), _vp]),
     "gs_batch_destroy": (_st, [_vp]),
     "gs_batch_info": (_st, [_vp, C.POINTER(UIN), C.POINTER(UIN), C.POINTER(C.c_double)]),

@@ -17,9 +17,15 @@
 // cudaSpmv.cu:723-737; nmc of a chunk is its first row's length, cudaSpmv.cu:744-749), so
 // the chunks that are split form a prefix 0..S-1.  A one-block
 // kernel finds S by bisection and writes the piece offsets of that prefix; the SpMV kernel
-// then runs split pieces first and every other chunk as one unit.  If the prefix would
-// not fit the scratch (nmc not sorted, or more than kStaticUnits pieces) nothing is split:
-// every chunk runs whole in one warp, which is slower but gives the same sums.  The host
+// then runs split pieces first and every other chunk as one unit.  With nmc out of order
+// the bisection still stops at some S: chunks before it are cut into pieces where they are
+// longer than one piece, and every chunk from S on runs whole in one warp, whatever its
+// length.  When the prefix does not fit the scratch (more than kStaticChunks chunks or
+// kStaticUnits pieces) nothing is split and every chunk runs whole.  Every case sums each
+// row correctly, but a row summed whole rounds differently from the same row summed in
+// pieces, so such results can differ in the last bits (within the FP64 error bound).
+// Pieces here are 256 steps long, where gs_spmv on a K1 matrix cuts at 128 steps: on rows
+// longer than 128 elements the two entry points also differ in the last bits.  The host
 // refuses layouts above GS_K1_STATIC_MAX_SLOTS slots, for which a sorted nmc could need
 // more pieces than the scratch holds.
 //

@@ -71,3 +71,25 @@ def vector(n: int, dist: str = "uniform", lo: float = -1.0, hi: float = 1.0, see
     L.check(L.lib().gs_gen_vector(n, 0 if dist == "uniform" else 1, lo, hi, seed,
                                   v.ctypes.data_as(L.FPTp)), "gs_gen_vector")
     return v
+
+
+def banded_batch(count: int = 256, seed: int = 3):
+    """The batched workload: `count` banded matrices with rows log-uniform in
+    [1000, 200000], half-bandwidth U[16, 256], U[5, 60] entries per row inside the band,
+    values N(0,1) (matrix i from seed 1000 * seed + i), each with U[1, 32] right-hand sides.
+    Returns a list of (row, col, val, k)."""
+    rng = np.random.default_rng(seed)
+    nrows = np.exp(rng.uniform(np.log(1000), np.log(200000), count)).astype(np.int64)
+    hbw = rng.integers(16, 257, count)
+    ks = rng.integers(1, 33, count)
+    out = []
+    for i in range(count):
+        row, col, val = banded(int(nrows[i]), int(hbw[i]), 5, 60, seed=1000 * seed + i)
+        out.append((row, col, val, int(ks[i])))
+    return out
+
+
+def batch_rhs(i: int, ncols: int, k: int, seed: int = 3, dtype=np.float32):
+    """Right-hand sides of matrix i of banded_batch: [ncols, k] N(0,1) entries."""
+    g = np.random.default_rng([seed, i])
+    return g.standard_normal((ncols, k)).astype(dtype)

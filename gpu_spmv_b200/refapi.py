@@ -74,3 +74,12 @@ def axc_arrays(a: L.StrMatAXC) -> dict:
 def axt_arrays(a: L.StrMatAXT) -> dict:
     return dict(ax=arr_f64(a.ax, a.lenAX), sec=arr_u32(a.sec, a.lenSEC),
                 con=arr_u32(a.con, a.lenCON + 1))
+
+
+def last_y(n: int) -> np.ndarray:
+    """y of this thread's most recent drop-in test_* product (row order)."""
+    out = np.zeros(n, np.float64)
+    got = L.lib().gs_dropin_last_y(f64p(out), n)
+    if got != n:
+        raise RuntimeError(f"the last drop-in product had {got} rows, expected {n}")
+    return out

@@ -231,6 +231,12 @@ const char *gs_version(void);
 /* Number of timed launches used by the drop-in test_* entry points (default 250). */
 void gs_set_num_ite(UIN num_ite);
 UIN gs_get_num_ite(void);
+/* The y of the calling thread's most recent drop-in test_* product (test_gcsr, test_gk1,
+ * test_gaxc, test_gaxt*, and their second-generation names), in row order, copied into
+ * out[0..n) when cap >= n; returns n (0 before any product).  No counterpart in the
+ * reference, whose test_* entry points only report get_errors' sign-blind summary: this
+ * lets a caller check every row of the product it timed. */
+UIN gs_dropin_last_y(FPT *out, UIN cap);
 
 /* Conversion parameters for gs_matrix_create.
  *  format  : GS_FMT_CSR / K1 / AXC / AXT
@@ -357,13 +363,6 @@ gs_status gs_copy_to_host(void *h_dst, const void *d_src, size_t bytes);
 gs_status gs_csr_spmv_f64(UIN nrows, UIN ncols, UIN nnz, const UIN *d_row, const UIN *d_col,
                           const double *d_val, const double *d_x, double *d_y,
                           gs_stream stream);
-
-/* Diagnostic (no counterpart in the reference): the rate of independent random 8-byte reads
- * from d_x[0..n) on this GPU, the ceiling of any SpMV whose x gathers hit random lines.  One
- * timed launch after a warm-up, every SM busy, `per_thread` reads per thread (a multiple of 8;
- * indices from a hash, all in range); *reads_per_s receives the rate.  Synchronises. */
-gs_status gs_gather_rate(const double *d_x, UIN n, UIN per_thread, double *reads_per_s,
-                         gs_stream stream);
 
 /* ---- multi-RHS products and the adjoint of y = A(v) x (K1 matrices, FP64 or FP32 values,
  * 32-bit columns).  No counterpart in the reference, which has one right-hand side and no

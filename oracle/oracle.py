@@ -49,11 +49,21 @@ def build_port(force: bool = False) -> str:
 
 
 def build_ref(ref_dir: str | None = None) -> bool:
-    """Compile the reference into oracle/_ref/ when its sources are present."""
-    ref_dir = ref_dir or os.environ.get("GS_REFERENCE_DIR", "/root/reference")
-    if not os.path.exists(os.path.join(ref_dir, "cudaSpmv.cu")):
+    """Compile the reference into oracle/_ref/ (``make -C oracle ref``) from the source tree
+    named by `ref_dir`, the GS_REFERENCE_DIR environment variable, or the recipe's REF_DIR.
+    A directory named here that holds no cudaSpmv.cu is an error; when the recipe's own
+    directory is absent (a machine without the reference), the prebuilt libraries are kept
+    and the result says whether they exist."""
+    ref_dir = ref_dir or os.environ.get("GS_REFERENCE_DIR")
+    cmd = ["make", "-s", "-C", HERE, "ref"]
+    if ref_dir:
+        if not os.path.exists(os.path.join(ref_dir, "cudaSpmv.cu")):
+            raise FileNotFoundError(f"reference directory {ref_dir} holds no cudaSpmv.cu")
+        cmd.append(f"REF_DIR={ref_dir}")
+        subprocess.run(cmd, check=True)
+        return True
+    if subprocess.run(cmd, stderr=subprocess.DEVNULL).returncode != 0:
         return os.path.exists(REF_SO)
-    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True)
     return True
 
 

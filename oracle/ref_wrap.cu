@@ -16,6 +16,7 @@
  *   ref_axt_*          -> getFormatDataAXT   (cudaSpmv.cu:1391-1566)
  *   ref_gpu_*          -> test_gcsr, test_gk1, test_gaxc, test_gaxtuh, test_gaxtuh1hw16w
  *                         (the reference's own GPU products, cudaSpmv.cu:547-2037)
+ *   ref_struct_layout  -> sizeof / offsetof of the reference's host-API structs
  *
  * No reference code is copied here: the wrappers only marshal arguments into the
  * reference's own structs (str_matCSR, str_matK1, str_matAXC, str_matAXT) and back out.
@@ -237,5 +238,47 @@ double ref_gpu_axt_uh1hw16(void *h, UIN wpw, UIN cbs, const FPT *ref, double *er
 {
     return res_out(test_gaxtuh1hw16w(wpw, cbs, *(str_matAXT *)h, ref), err3); /* :1603 */
 }
+
+/* sizeof and the offset of every field of the reference's host-API structs, in the order
+ * of their declarations (cudaSpmv.cu:261, 385, 470, 499, 712, 933, 1154), as "name value"
+ * lines; returns the number of characters written (0 if cap is too small). */
+#define REF_SZ(T) n += snprintf(buf + n, cap > n ? cap - n : 0, #T " %zu\n", sizeof(T))
+#define REF_OF(T, f) n += snprintf(buf + n, cap > n ? cap - n : 0, #T "." #f " %zu\n", offsetof(T, f))
+size_t ref_struct_layout(char *buf, size_t cap)
+{
+    size_t n = 0;
+    REF_SZ(str_matCSR);
+    REF_OF(str_matCSR, name); REF_OF(str_matCSR, nrows); REF_OF(str_matCSR, nnz);
+    REF_OF(str_matCSR, rmin); REF_OF(str_matCSR, rave); REF_OF(str_matCSR, rmax);
+    REF_OF(str_matCSR, rsd); REF_OF(str_matCSR, bw); REF_OF(str_matCSR, val);
+    REF_OF(str_matCSR, row); REF_OF(str_matCSR, rowStart); REF_OF(str_matCSR, rowEnd);
+    REF_OF(str_matCSR, col); REF_OF(str_matCSR, rl);
+    REF_SZ(str_formatData);
+    REF_OF(str_formatData, name); REF_OF(str_formatData, mfp); REF_OF(str_formatData, beta);
+    REF_OF(str_formatData, ct);
+    REF_SZ(str_err);
+    REF_OF(str_err, aErr); REF_OF(str_err, rErr); REF_OF(str_err, pos);
+    REF_SZ(str_res);
+    REF_OF(str_res, name); REF_OF(str_res, et); REF_OF(str_res, ot); REF_OF(str_res, flops);
+    REF_OF(str_res, sErr);
+    REF_SZ(str_matK1);
+    REF_OF(str_matK1, nrows); REF_OF(str_matK1, nnz); REF_OF(str_matK1, chunkNum);
+    REF_OF(str_matK1, lenVC); REF_OF(str_matK1, permi); REF_OF(str_matK1, nmc);
+    REF_OF(str_matK1, chp); REF_OF(str_matK1, val); REF_OF(str_matK1, col);
+    REF_SZ(str_matAXC);
+    REF_OF(str_matAXC, nrows); REF_OF(str_matAXC, nnz); REF_OF(str_matAXC, hbs);
+    REF_OF(str_matAXC, lenAX); REF_OF(str_matAXC, lenBRP); REF_OF(str_matAXC, lenMAPX);
+    REF_OF(str_matAXC, ax); REF_OF(str_matAXC, brp); REF_OF(str_matAXC, mapx);
+    REF_SZ(str_matAXT);
+    REF_OF(str_matAXT, name); REF_OF(str_matAXT, nrows); REF_OF(str_matAXT, nnz);
+    REF_OF(str_matAXT, mode); REF_OF(str_matAXT, tileHW); REF_OF(str_matAXT, tileH);
+    REF_OF(str_matAXT, logTH); REF_OF(str_matAXT, tileN); REF_OF(str_matAXT, lenAX);
+    REF_OF(str_matAXT, lenSEC); REF_OF(str_matAXT, lenCON); REF_OF(str_matAXT, log);
+    REF_OF(str_matAXT, bs); REF_OF(str_matAXT, ax); REF_OF(str_matAXT, sec);
+    REF_OF(str_matAXT, con);
+    return n < cap ? n : 0;
+}
+#undef REF_SZ
+#undef REF_OF
 
 }  // extern "C"

@@ -51,8 +51,6 @@ def test_argument_errors_need_no_gpu():
     assert lib.gs_spmv(None, None, 0, None, 0, 0, None) == L.GS_ERR_INVALID
     assert lib.gs_matrix_get_info(None, None) == L.GS_ERR_INVALID
     assert b"NULL" in lib.gs_last_error()
-    r = C.c_double()
-    assert lib.gs_gather_rate(None, 16, 8, C.byref(r), None) == L.GS_ERR_INVALID
 
 
 @pytest.mark.parametrize("case,expect", [
@@ -128,3 +126,59 @@ def test_gen2_struct_layouts_and_names(tmp_path):
     assert int(out["axc"]) == C.sizeof(L.Gen2MatAXC)
     assert int(out["axt"]) == C.sizeof(L.Gen2MatAXT)
     assert int(out["axt_con"]) == L.Gen2MatAXT.con.offset
+
+
+def test_reference_arm_loads_no_engine_code():
+    """bench.py --impl reference times the reference's own CPU SpMV on inputs from the
+    oracle-side generator: no library of the engine package may be mapped into it."""
+    import json
+    import subprocess
+    import sys
+
+    from oracle.oracle import Ref
+
+    if not Ref.available():
+        pytest.skip("reference oracle library oracle/_ref not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--workload", "laplacian", "--steps", "3", "--warmup", "3"],
+                         capture_output=True, text=True, check=True, timeout=600)
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    libs = line["loaded_libraries"]
+    assert any(p.startswith("oracle/") for p in libs), libs
+    assert not any(p.startswith("gpu_spmv_b200/") for p in libs), libs
+
+
+def test_struct_layouts_match_compiled_reference(tmp_path):
+    """sizeof and every field offset of the drop-in header's str_matCSR, str_formatData,
+    str_err, str_res, str_matK1, str_matAXC and str_matAXT equal those of the reference's own
+    structs (cudaSpmv.cu:261, 385, 470, 499, 712, 933, 1154) as its compiled source lays them
+    out (oracle/_ref/libref_oracle.so)."""
+    from oracle.oracle import REF_SO, Ref
+
+    if not Ref.available():
+        pytest.skip("reference oracle library oracle/_ref not built")
+    ref = C.CDLL(REF_SO)
+    ref.ref_struct_layout.restype = C.c_size_t
+    ref.ref_struct_layout.argtypes = [C.c_char_p, C.c_size_t]
+    buf = C.create_string_buffer(1 << 14)
+    assert ref.ref_struct_layout(buf, len(buf)) > 0
+    want = dict(l.split() for l in buf.value.decode().splitlines())
+    prog = tmp_path / "lay.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
+             "int main(void){"]
+    for key in want:
+        if "." in key:
+            t, f = key.split(".")
+            lines.append(f'printf("{key} %zu\\n", offsetof({t}, {f}));')
+        else:
+            lines.append(f'printf("{key} %zu\\n", sizeof({key}));')
+    lines.append("return 0;}")
+    prog.write_text("\n".join(lines))
+    exe = tmp_path / "lay"
+    subprocess.run(["gcc", str(prog), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                  check=True).stdout.splitlines())
+    assert len(want) == 67  # 7 sizes, 60 field offsets
+    assert got == want

@@ -87,3 +87,74 @@ def test_laplacian_512(port):
         if kw["fmt"] == "K1":
             assert np.array_equal(y, port.csr_spmv(row, col, val, x))
         A.close()
+
+
+@pytest.mark.parametrize("fmt", [dict(fmt="K1"),
+                                 dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
+                                 dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256)],
+                         ids=["k1", "unc4", "com1"])
+def test_powerlaw_64M_conversion_bit_exact(port, powerlaw, fmt):
+    """The device converters on the headline matrix (4,194,304 rows, 67,108,864 nnz)
+    against the oracle's restated converters, which the CPU suite pins to the reference's
+    own at this size: K1 permi / nmc / chp / val / col (the stable length sort of 4M rows
+    with heavy ties, cudaSpmv.cu:716-846), AXT sec / con and the value and column slots
+    (cudaSpmv.cu:1158-1566), bit for bit."""
+    from gpu_spmv_b200 import engine as E
+
+    row, col, val, x = powerlaw
+    n = len(row) - 1
+    A = E.Matrix(row, col, val, ncols=n, keep_layout=True, **fmt)
+    lay = A.layout()
+    i = A.info
+    if fmt["fmt"] == "K1":
+        k = port.k1(row, col, val)
+        assert (i.chunkNum, i.lenVC) == (k["chunkNum"], k["lenVC"])
+        for key in ("permi", "nmc", "chp", "val", "col"):
+            assert np.array_equal(lay[key], k[key]), key
+    else:
+        t = port.axt(row, col, val, fmt["tileHW"], fmt["tileH"], fmt["mode"],
+                     bs=fmt.get("bs", 256))
+        d = t["dims"]
+        assert (i.tileN, i.lenAX, i.lenSEC, i.lenCON, i.log, i.logTH) == \
+            (d.tileN, d.lenAX, d.lenSEC, d.lenCON, d.log, d.logTH)
+        for key in ("val", "col", "sec", "con"):
+            assert np.array_equal(lay[key], t[key]), key
+    del lay
+    # and the product from the converted layout
+    _check(port, row, col, val, x, A.spmv(torch.from_numpy(x).cuda()).cpu().numpy())
+    A.close()
+
+
+@pytest.mark.parametrize("fmt", [dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
+                                 dict(fmt="AXT", mode="COM", tileH=8, tileHW=32, bs=256),
+                                 dict(fmt="AXC", hbs=32),
+                                 dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4)],
+                         ids=["unc8", "com8", "axc", "unc1hw4"])
+def test_powerlaw_64M_other_formats(port, powerlaw, fmt):
+    """Row-stream layouts with 8 positions per lane and ~2048-position warp ranges, and the
+    tile kernel, on the full power-law matrix: within 1e-13 (|A||x|)_i of the oracle."""
+    from gpu_spmv_b200 import engine as E
+
+    row, col, val, x = powerlaw
+    n = len(row) - 1
+    A = E.Matrix(row, col, val, ncols=n, **fmt)
+    _check(port, row, col, val, x, A.spmv(torch.from_numpy(x).cuda()).cpu().numpy())
+    A.close()
+
+
+def test_stencil27_160_row_stream(port):
+    """CSR (8 positions per lane: the stencil's columns are local) and AXT COM tileH 1 on
+    the 27-point stencil 160^3 against the oracle."""
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    row, col, val = matgen.stencil27(160, seed=2)
+    n = len(row) - 1
+    x = matgen.vector(n, "normal", seed=2)
+    for kw in (dict(fmt="CSR"), dict(fmt="AXT", mode="COM", tileH=1, tileHW=32),
+               dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32)):
+        A = E.Matrix(row, col, val, ncols=n, **kw)
+        if kw["fmt"] == "CSR":
+            assert A.info.lane_positions == 8
+        _check(port, row, col, val, x, A.spmv(torch.from_numpy(x).cuda()).cpu().numpy())
+        A.close()

@@ -129,3 +129,75 @@ def test_dropin_errors_do_not_exit(lib):
     fd = lib.getFormatDataAXT(1, 256, 32, 1, b"COM", h.s, R.f64p(np.zeros(1)), C.byref(t))
     res = lib.test_gaxtuh1hw16w(64, 256, t, R.f64p(np.zeros(1)))
     assert res.name == b"error"
+
+
+def _dropin_inputs(name):
+    rng = np.random.default_rng(7)
+    if name.endswith(".npz"):
+        g = np.load(name)
+        row, col, val = g["row"], g["col"], g["val"]
+        x = np.arange(len(row) - 1, dtype=np.float64)  # init_vec: x[i] = i
+    else:
+        row, col, val = case(name, rng)
+        x = rng.uniform(-1, 1, len(row) - 1)
+    return row, col, val, x
+
+
+@pytest.mark.parametrize("name", GOLDEN + ["powerlaw_small", "mixed", "dense_row"],
+                         ids=[os.path.basename(p) for p in GOLDEN] +
+                         ["powerlaw_small", "mixed", "dense_row"])
+def test_dropin_products_per_row_and_metrics(lib, port, ref, name):
+    """Every drop-in test_* entry point's y, read back row by row, within
+    1e-13 (|A||x|)_i of the reference's CPU loop with its sign (get_errors compares
+    magnitudes only, cudaSpmv.cu:474-495); and every converter's format metrics (name, mfp,
+    beta) equal to the compiled reference's getFormatData* (cudaSpmv.cu:826-845, 1050-1061,
+    1558-1565)."""
+    from gpu_spmv_b200 import _lib as L
+    from gpu_spmv_b200 import refapi as R
+
+    row, col, val, x = _dropin_inputs(name)
+    n = len(row) - 1
+    h = R.csr_struct(row, col, val)
+    y_ref = port.csr_spmv(row, col, val, x)
+    _, mag = port.csr_truth(row, col, val, x)
+
+    def check(res, what):
+        assert res.name != b"error", (what, lib.gs_last_error())
+        y = R.last_y(n)
+        err = np.abs(y - y_ref)
+        assert np.all(err <= 1e-13 * mag), (what, float(np.max(err / np.maximum(mag, 1e-300))))
+
+    check(lib.test_gcsr(256, h.s, R.f64p(x), R.f64p(y_ref)), "gcsr")
+
+    k = L.StrMatK1()
+    fd = lib.getFormatDataK1(32, h.s, R.f64p(x), C.byref(k))
+    rk = ref.k1(row, col, val, x)
+    assert (fd.name, fd.mfp, fd.beta) == (b"fk1", rk["fd"][0], rk["fd"][1])
+    check(lib.test_gk1(256, k, R.f64p(x), R.f64p(y_ref)), "gk1")
+    R.free_struct_arrays(k, ("permi", "nmc", "chp", "val", "col"))
+
+    a = L.StrMatAXC()
+    fd = lib.getFormatDataAXC(1, 32, h.s, R.f64p(x), C.byref(a))
+    ra = ref.axc(row, col, val, x, hbs=32)
+    assert (fd.name, fd.mfp, fd.beta) == (b"faxc", ra["fd"][0], ra["fd"][1])
+    check(lib.test_gaxc(256, a, R.f64p(y_ref)), "gaxc")
+    R.free_struct_arrays(a, ("ax", "brp", "mapx"))
+
+    for (mode, th, thw, bs) in AXT_PARAMS:
+        t = L.StrMatAXT()
+        fd = lib.getFormatDataAXT(1, bs, thw, th, mode.encode(), h.s, R.f64p(x), C.byref(t))
+        rt = ref.axt(row, col, val, x, thw, th, mode, bs=bs)
+        key = (mode, th, thw, bs)
+        assert fd.name.decode() == rt["name"], key
+        assert (fd.mfp, fd.beta) == (rt["fd"][0], rt["fd"][1]), key
+        if mode == "UNC" and th == 1:
+            fn = {16: lib.test_gaxtuh1hw16w, 8: lib.test_gaxtuh1hw08w, 4: lib.test_gaxtuh1hw04w}
+            res = fn.get(thw, lib.test_gaxtuh1hw16w)(128, 256, t, R.f64p(y_ref))
+        elif mode == "UNC":
+            res = lib.test_gaxtuh(2, 256, t, R.f64p(y_ref))
+        elif th == 1:
+            res = lib.test_gaxtch1(bs, t, R.f64p(y_ref))
+        else:
+            res = lib.test_gaxtch(256, t, R.f64p(y_ref))
+        check(res, key)
+        R.free_struct_arrays(t, ("ax", "sec", "con"))

@@ -64,3 +64,22 @@ def test_vector_seeded():
     assert np.array_equal(a, b) and a.min() >= -1 and a.max() < 1
     z = matgen.vector(100000, "normal", seed=4)
     assert abs(z.mean()) < 0.02 and abs(z.std() - 1) < 0.02
+
+
+def test_reference_arm_generator_same_bytes():
+    """The reference arm of bench.py builds its inputs with oracle/_build/libgs_workload.so
+    (the same generator source built apart from the engine library): the same seed must give
+    the same bytes as the engine's generator, for the headline power-law configuration
+    (4,194,304 rows, 67,108,864 nnz, seed 1, x seed 1001) and the other workloads."""
+    from oracle import workload as W
+
+    for a, b in ((matgen.powerlaw(seed=1), W.powerlaw(seed=1)),
+                 (matgen.stencil27(40, seed=2), W.stencil27(40, seed=2)),
+                 (matgen.laplacian2d(64), W.laplacian2d(64)),
+                 (matgen.banded(3000, 100, 5, 60, seed=3001), W.banded(3000, 100, 5, 60, seed=3001))):
+        for u, v in zip(a, b):
+            assert u.dtype == v.dtype and np.array_equal(u.view(np.uint8), v.view(np.uint8))
+    for dist, seed in (("uniform", 1001), ("normal", 2)):
+        u = matgen.vector(4194304, dist, -1.0, 1.0, seed=seed)
+        v = W.vector(4194304, dist, -1.0, 1.0, seed=seed)
+        assert np.array_equal(u.view(np.uint8), v.view(np.uint8))

@@ -119,3 +119,30 @@ def test_com_row0_header_is_zero(port):
     assert t["sec"][0] == 0
     x = np.array([1.0, 2.0, 3.0])
     assert np.array_equal(port.axt_spmv(t, x), port.csr_spmv(row, col, val, x))
+
+
+@pytest.fixture(scope="module")
+def powerlaw_64m():
+    from gpu_spmv_b200 import matgen
+
+    row, col, val = matgen.powerlaw(seed=1)
+    x = matgen.vector(len(row) - 1, "uniform", -1.0, 1.0, seed=1001)
+    return row, col, val, x
+
+
+def test_restatement_equals_reference_at_benchmark_size(port, ref, powerlaw_64m):
+    """The restated converters against the reference's own (compiled unchanged) on the
+    headline power-law matrix, 4,194,304 rows and 67,108,864 nnz: K1 (cudaSpmv.cu:716-846,
+    a stable sort of 4M rows with heavy length ties), AXT UNC tileH 4 and COM tileH 1
+    (cudaSpmv.cu:1158-1566), bit for bit."""
+    row, col, val, x = powerlaw_64m
+    k_ref = ref.k1(row, col, val, x)
+    k = port.k1(row, col, val)
+    for f in ("permi", "nmc", "chp", "val", "col"):
+        assert np.array_equal(k[f], k_ref[f]), f
+    del k_ref, k
+    for thw, th, mode in ((32, 4, "UNC"), (32, 1, "COM")):
+        a_ref = ref.axt(row, col, val, x, thw, th, mode, threads=os.cpu_count() or 1)
+        a = port.axt(row, col, val, thw, th, mode, x=x)
+        for f in ("ax", "sec", "con"):
+            assert np.array_equal(a[f], a_ref[f]), (mode, th, f)
