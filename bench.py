@@ -398,10 +398,11 @@ def time_adjoint(steps: int):
 
     vslots = torch.empty(A.value_slots(), device="cuda")
 
-    def adj(mode, order):
+    def adj(mode, order, want_vbar=True):
         vb = vslots if order == L.GS_VALUES_SLOTS else vbar
         L.check(lib.gs_spmm_adjoint(A._h, Yb.data_ptr(), X.data_ptr(), Xbar.data_ptr(),
-                                    vb.data_ptr(), L.GS_F32, k, mode, order, sh), "adjoint")
+                                    vb.data_ptr() if want_vbar else None, L.GS_F32, k, mode,
+                                    order, sh), "adjoint")
 
     vals = torch.from_numpy(val.astype(np.float32)).cuda()
     vals_slots = A.convert_values(vals, to="slots")
@@ -409,6 +410,9 @@ def time_adjoint(steps: int):
     ads = _time_us(lambda: adj(L.GS_ADJ_DETERMINISTIC, L.GS_VALUES_SLOTS), steps)
     adc = _time_us(lambda: adj(L.GS_ADJ_DETERMINISTIC, L.GS_VALUES_CSR), steps)
     aa = _time_us(lambda: adj(L.GS_ADJ_ATOMIC, L.GS_VALUES_CSR), steps)
+    aas = _time_us(lambda: adj(L.GS_ADJ_ATOMIC, L.GS_VALUES_SLOTS), steps)
+    ax_d = _time_us(lambda: adj(L.GS_ADJ_DETERMINISTIC, L.GS_VALUES_CSR, False), steps)
+    ax_a = _time_us(lambda: adj(L.GS_ADJ_ATOMIC, L.GS_VALUES_CSR, False), steps)
     svs = _time_us(lambda: A.set_values(vals_slots, "slots"), steps)
     svc = _time_us(lambda: A.set_values(vals, "csr"), steps)
     A.close()
@@ -417,10 +421,14 @@ def time_adjoint(steps: int):
             "adjoint_deterministic_slots_us": round(ads, 2),
             "adjoint_deterministic_csr_us": round(adc, 2),
             "adjoint_atomic_csr_us": round(aa, 2),
+            "adjoint_atomic_slots_us": round(aas, 2),
+            "xbar_only_deterministic_us": round(ax_d, 2),
+            "xbar_only_atomic_us": round(ax_a, 2),
             "set_values_slots_us": round(svs, 2), "set_values_csr_us": round(svc, 2),
             "fwd_plus_adj_over_fwd": round((f + ads) / f, 3),
             "fwd_plus_adj_over_fwd_csr_order": round((f + adc) / f, 3),
             "fwd_plus_adj_over_fwd_atomic": round((f + aa) / f, 3),
+            "fwd_plus_xbar_over_fwd_atomic": round((f + ax_a) / f, 3),
             "note": "adjoint = Xbar = A^T Ybar and vbar (value gradient) in one launch; "
                     "slots = values kept in the adjoint layout's order"}
 
@@ -598,13 +606,18 @@ def gather4_rates(dx, n, per_lane: int = 256):
     lib = probe_lib()
     out = {}
     n2 = n & ~1
-    for warps, lsu, bps in ((4, 0, 2), (8, 0, 2), (8, 0, 3), (8, 4, 2), (8, 2, 2), (8, 8, 2)):
+    # (warps per block, of which load-path warps, blocks per SM): 16 KB of stages per
+    # gather4 warp, so at most 12 gather4 warps per SM
+    for warps, lsu, bps in ((4, 0, 3), (8, 0, 1), (4, 0, 2), (4, 2, 3), (8, 4, 1), (8, 4, 2),
+                            (8, 8, 2)):
         rate, to = Cc.c_double(), Cc.c_uint32()
         if lib.gsp_gather4_rate(dx.data_ptr(), n2, per_lane, warps, lsu, bps, Cc.byref(rate),
                                 Cc.byref(to), None):
             raise RuntimeError(f"gsp_gather4_rate: {lib.gsp_last_error().decode()}")
         if to.value:
-            raise RuntimeError("gsp_gather4_rate: a bounded wait gave up")
+            raise RuntimeError("gsp_gather4_rate: " + ("a destination was not 128-byte aligned"
+                                                       if to.value & 2 else
+                                                       "a bounded wait gave up"))
         out[f"{bps}x{warps}warps_{lsu}lsu"] = rate.value
     return out
 

@@ -66,7 +66,7 @@ class _SpMM(torch.autograd.Function):
         v, X = ctx.saved_tensors
         op = ctx.op
         op.ensure_values(v, ctx.order)  # the operator may have seen other values since
-        want_v = ctx.needs_input_grad[0] or ctx.mode == "atomic"
+        want_v = ctx.needs_input_grad[0]
         Xbar, vbar = op.mat.adjoint(Ybar.contiguous(), X if want_v else None, mode=ctx.mode,
                                     want_vbar=want_v, order=ctx.order)
         return ((vbar if ctx.needs_input_grad[0] else None),

@@ -63,8 +63,11 @@ __global__ void __launch_bounds__(256) k_gather_rate(const double *__restrict__ 
     if (acc == 1.2345678e300) sink[0] = acc;  // never true for finite x: keeps the reads
 }
 
-constexpr int kG4Stages = 4;          // stages per warp
-constexpr uint32_t kG4StageBytes = 32u * 64u;  // 32 lanes x one gather4 (4 rows x 16 bytes)
+constexpr int kG4Stages = 4;            // stages per warp
+constexpr uint32_t kG4Bytes = 64u;       // one gather4: 4 rows x 16 bytes
+constexpr uint32_t kG4Slot = 128u;       // a tensor copy's shared-memory destination is
+                                         // 128-byte aligned: one slot per lane
+constexpr uint32_t kG4StageBytes = 32u * kG4Slot;
 
 __device__ __forceinline__ void gather4(void *dst, const CUtensorMap *tm, int32_t c, int32_t r0,
                                         int32_t r1, int32_t r2, int32_t r3, uint64_t *bar)
@@ -105,9 +108,11 @@ __global__ void __launch_bounds__(256) k_gather4_rate(const __grid_constant__ CU
             for (int b = 0; b < 8; b++) acc += v[b];
         }
     } else {
-        unsigned char *buf = smem + (size_t)wid * kG4Stages * kG4StageBytes;
-        uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)nw * kG4Stages * kG4StageBytes) +
-                         wid * kG4Stages;
+        const uint32_t tw = (uint32_t)wid - lsu_warps;  // index among the gather4 warps
+        unsigned char *buf = smem + (size_t)tw * kG4Stages * kG4StageBytes;
+        uint64_t *bars = reinterpret_cast<uint64_t *>(
+                             smem + (size_t)(nw - lsu_warps) * kG4Stages * kG4StageBytes) +
+                         tw * kG4Stages;
         if (lane == 0)
             for (int i = 0; i < kG4Stages; i++) gs::bulk::mbar_init(bars + i, 1);
         gs::bulk::fence_mbar_init();
@@ -122,10 +127,16 @@ __global__ void __launch_bounds__(256) k_gather4_rate(const __grid_constant__ CU
                 ok = gs::bulk::mbar_wait_bounded(bars + st, ((it / kG4Stages) - 1u) & 1u);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
-                acc += *reinterpret_cast<const double *>(buf + st * kG4StageBytes + lane * 64);
+                acc += *reinterpret_cast<const double *>(buf + st * kG4StageBytes + lane * kG4Slot);
+            }
+            unsigned char *dst = buf + st * kG4StageBytes + lane * kG4Slot;
+            // a misaligned destination is recorded and the stage skipped, never issued
+            if (!__all_sync(0xffffffffu, (gs::bulk::smem_addr(dst) & 127u) == 0u)) {
+                if (lane == 0) atomicOr(status, 2u);
+                break;
             }
             __syncwarp();
-            if (lane == 0) gs::bulk::mbar_expect_tx(bars + st, kG4StageBytes);
+            if (lane == 0) gs::bulk::mbar_expect_tx(bars + st, 32u * kG4Bytes);
             __syncwarp();
             int32_t r[4];
 #pragma unroll
@@ -133,7 +144,7 @@ __global__ void __launch_bounds__(256) k_gather4_rate(const __grid_constant__ CU
                 s = mix32(s + (uint32_t)b);
                 r[b] = (int32_t)(s % nrow2);
             }
-            gather4(buf + st * kG4StageBytes + lane * 64, &tm, 0, r[0], r[1], r[2], r[3], bars + st);
+            gather4(dst, &tm, 0, r[0], r[1], r[2], r[3], bars + st);
             issued = it + 1;
         }
         // drain: every stage still in flight (bounded; a second limit after a timeout)
@@ -141,7 +152,7 @@ __global__ void __launch_bounds__(256) k_gather4_rate(const __grid_constant__ CU
         for (uint32_t it = first; it < issued; it++) {
             const int st = (int)(it % kG4Stages);
             if (!gs::bulk::mbar_wait_bounded(bars + st, (it / kG4Stages) & 1u)) ok = false;
-            else acc += *reinterpret_cast<const double *>(buf + st * kG4StageBytes + lane * 64);
+            else acc += *reinterpret_cast<const double *>(buf + st * kG4StageBytes + lane * kG4Slot);
         }
         if (!ok && lane == 0) atomicOr(status, 1u);
     }
@@ -241,7 +252,8 @@ int gsp_gather4_rate(const double *d_x, uint32_t n, uint32_t per_lane, uint32_t 
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return fail("device query", e);
-    const size_t smem = (size_t)warps * kG4Stages * kG4StageBytes + (size_t)warps * kG4Stages * 8;
+    const size_t tw = warps - lsu_warps;
+    const size_t smem = tw * kG4Stages * kG4StageBytes + tw * kG4Stages * 8 + 8;
     e = cudaFuncSetAttribute(k_gather4_rate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return fail("cudaFuncSetAttribute", e);
     const unsigned blocks = (unsigned)sms * blocks_per_sm;

@@ -171,6 +171,10 @@ struct gs_matrix {
     bool mm_ready = false, adj_ready = false;
     gs::DevBuf fsrc;    // forward slot -> CSR index
     gs::DevBuf ftslot;  // forward slot -> adjoint-layout slot
+    gs::DevBuf csr2t;   // CSR index -> adjoint-layout slot
+    gs::DevBuf csr2f;   // CSR index -> forward slot
+    gs::DevBuf t2f;     // adjoint-layout slot -> forward slot (padding: none)
+    gs::DevBuf vslots;  // vbar in slot order before it is gathered into CSR order
     gs::DevBuf tpermi, tnmc, tchp, tlen, trow, tsrc, tval;  // K1 layout of A^T
     gs::DevBuf tunit_chunk, tunit_base, tpartial1, tcount, tpartial;
     uint32_t tchunkNum = 0, tlenVC = 0, tunits = 0, tsplit_units = 0;

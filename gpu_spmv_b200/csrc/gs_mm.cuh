@@ -119,12 +119,11 @@ struct MMArgs {
     const uint32_t *permi, *nmc, *chp, *klen;  // K1 layout
     const void *val;
     const uint32_t *col;                       // gathered row index (A: col, A^T: row of A)
-    const uint32_t *src;                       // A^T only: CSR index of each slot
     const void *xin;                           // gathered operand (A: X, A^T: Ybar)
     const void *xrow;                          // A^T only: X, row j held for vbar
     void *yout;                                // A: Y, A^T: Xbar
-    void *vbar;                                // A^T only, or nullptr
-    bool vbar_slots;                           // vbar in this layout's slot order
+    void *vbar;                                // A^T only, or nullptr: vbar in this
+                                               // layout's slot order, padding slots zero
     const uint32_t *unit_chunk, *unit_base;
     uint32_t units, split_units;               // units < split_units may be pieces
     void *partial;                             // split_units * ld * 32 values
@@ -170,15 +169,13 @@ __device__ __forceinline__ void mm_unit(const MMArgs &a, uint32_t u, uint32_t rb
         for (int k = 0; k < K; k++) acc[k] = T(0);
         for (uint32_t j = j0; j < j1; j += B) {
             T v[B], gv[B][K];
-            uint32_t cc[B], sr[B];
+            uint32_t cc[B];
 #pragma unroll
             for (int b = 0; b < B; b++) {
                 const bool in = j + b < j1;
                 const uint32_t pos = base + 32u * (j + b);
                 v[b] = in ? __ldcs(val + pos) : T(0);
                 cc[b] = in ? __ldcs(a.col + pos) : 0u;
-                if constexpr (ADJ)
-                    sr[b] = (in && a.vbar && !a.vbar_slots) ? __ldcs(a.src + pos) : kNoSrc;
             }
 #pragma unroll
             for (int b = 0; b < B; b++) {
@@ -203,8 +200,7 @@ __device__ __forceinline__ void mm_unit(const MMArgs &a, uint32_t u, uint32_t rb
                             T d = T(0);
 #pragma unroll
                             for (int k = 0; k < K; k++) d = A::add(d, A::mul(gv[b][k], xr[k]));
-                            static_cast<T *>(a.vbar)[a.vbar_slots ? base + 32u * (j + b)
-                                                                  : sr[b]] = d;
+                            static_cast<T *>(a.vbar)[base + 32u * (j + b)] = d;
                         }
                     }
                 }
@@ -212,7 +208,7 @@ __device__ __forceinline__ void mm_unit(const MMArgs &a, uint32_t u, uint32_t rb
         }
         if constexpr (ADJ) {
             // slot order: this piece's padding slots of the lane get a zero gradient
-            if (a.vbar && a.vbar_slots) {
+            if (a.vbar) {
                 const uint32_t pend = min(__ldg(a.nmc + c), j0 + kK1Split);
                 for (uint32_t j = max(j0, len); j < pend; j++)
                     static_cast<T *>(a.vbar)[base + 32u * j] = T(0);

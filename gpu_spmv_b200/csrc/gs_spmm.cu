@@ -38,15 +38,15 @@ __global__ void __launch_bounds__(256) k_k1_mm(const MMArgs a)
 }
 
 // Atomic-mode adjoint on the forward layout, over the same kK1Split-step work units: lane = row
-// r of A with Ybar[r] in registers; per stored element e: vbar_e = Ybar[r] . X[col_e] and
-// Xbar[col_e] += v_e Ybar[r] (atomic adds; Xbar zeroed first).
+// r of A with Ybar[r] in registers; per stored element e: Xbar[col_e] += v_e Ybar[r] (atomic
+// adds; Xbar zeroed first) and, when vbar is wanted, vbar_e = Ybar[r] . X[col_e] (one more
+// gather of X's row per element).
 struct AtomicArgs {
     uint32_t nrows;
     const uint32_t *permi, *chp, *klen, *col, *unit_chunk, *unit_base;
-    const uint32_t *vidx;  // forward slot -> vbar index (CSR index or adjoint-layout slot)
     uint32_t units;
     const void *val, *x, *ybar;
-    void *xbar, *vbar;
+    void *xbar, *vbar;  // vbar (or nullptr) in forward slot order
 };
 
 template <class T, int K>
@@ -95,22 +95,26 @@ __global__ void __launch_bounds__(256) k_k1_adj_atomic(const AtomicArgs a)
                 const uint32_t pos = base + 32u * (j + b);
                 v[b] = in ? __ldcs(val + pos) : T(0);
                 cc[b] = in ? __ldcs(a.col + pos) : 0u;
-                sr[b] = in ? __ldcs(a.vidx + pos) : kNoSrc;
+                sr[b] = pos;  // vbar in forward slot order
             }
+            if (vbar) {
 #pragma unroll
-            for (int b = 0; b < B; b++) {
-                if (j + b < j1) load_row<T, K>(x, cc[b], K, xg[b]);
+                for (int b = 0; b < B; b++) {
+                    if (j + b < j1) load_row<T, K>(x, cc[b], K, xg[b]);
+                }
             }
 #pragma unroll
             for (int b = 0; b < B; b++) {
                 if (j + b < j1) {
-                    T d = T(0), contrib[K];
+                    T contrib[K];
 #pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        d = A::add(d, A::mul(yb[k], xg[b][k]));
-                        contrib[k] = A::mul(v[b], yb[k]);
+                    for (int k = 0; k < K; k++) contrib[k] = A::mul(v[b], yb[k]);
+                    if (vbar) {
+                        T d = T(0);
+#pragma unroll
+                        for (int k = 0; k < K; k++) d = A::add(d, A::mul(yb[k], xg[b][k]));
+                        vbar[sr[b]] = d;
                     }
-                    vbar[sr[b]] = d;
                     red_row<T, K>(static_cast<T *>(a.xbar), cc[b], contrib);
                 }
             }
@@ -467,14 +471,21 @@ gs_status gs_matrix_prepare_adjoint(gs_matrix *A, const UIN *d_row, const UIN *d
                                                 vcsr.as<float>(), A->tval.as<float>());
     }
     GS_CHECK_LAUNCH();
-    // forward slot -> adjoint-layout slot, through the CSR index
-    DevBuf csr2t;
-    GS_TRY(csr2t.alloc((size_t)nnz * 4 + 4));
+    // forward slot -> adjoint-layout slot, through the CSR index; the CSR index -> slot maps
+    // stay: a value gradient in CSR order is formed in slot order (coalesced writes) and then
+    // gathered into CSR order, instead of scattering one 4- or 8-byte write per element
+    GS_TRY(A->csr2t.alloc((size_t)nnz * 4 + 4));
+    GS_TRY(A->csr2f.alloc((size_t)nnz * 4 + 4));
     GS_TRY(A->ftslot.alloc((size_t)A->lenVC * 4 + 4));
-    k_invert_map<<<gb, 256, 0, s>>>(A->tlenVC, A->tsrc.as<uint32_t>(), csr2t.as<uint32_t>());
-    k_compose_map<<<gb, 256, 0, s>>>(A->lenVC, A->fsrc.as<uint32_t>(), csr2t.as<uint32_t>(),
+    k_invert_map<<<gb, 256, 0, s>>>(A->tlenVC, A->tsrc.as<uint32_t>(), A->csr2t.as<uint32_t>());
+    k_invert_map<<<gb, 256, 0, s>>>(A->lenVC, A->fsrc.as<uint32_t>(), A->csr2f.as<uint32_t>());
+    k_compose_map<<<gb, 256, 0, s>>>(A->lenVC, A->fsrc.as<uint32_t>(), A->csr2t.as<uint32_t>(),
                                      A->ftslot.as<uint32_t>());
+    GS_TRY(A->t2f.alloc((size_t)A->tlenVC * 4 + 4));
+    k_compose_map<<<gb, 256, 0, s>>>(A->tlenVC, A->tsrc.as<uint32_t>(), A->csr2f.as<uint32_t>(),
+                                     A->t2f.as<uint32_t>());
     GS_CHECK_LAUNCH();
+    GS_TRY(A->vslots.alloc((size_t)max(A->lenVC, A->tlenVC) * vsz + 8));
     A->adj_ready = true;
     GS_CUDA(cudaStreamSynchronize(s));
     return GS_OK;
@@ -555,8 +566,8 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
         return fail(GS_ERR_INVALID, "Ybar, X and Xbar must be 32-byte aligned");
     cudaStream_t s = cs(stream);
     const bool f64 = A->p.vtype == GS_F64;
+    const unsigned gb = 148u * 16u;
     if (mode == GS_ADJ_ATOMIC) {
-        if (!d_vbar || !d_X) return fail(GS_ERR_INVALID, "the atomic mode computes vbar: pass X and vbar");
         GS_CUDA(cudaMemsetAsync(d_Xbar, 0, (size_t)A->ncols * k * (f64 ? 8 : 4), s));
         AtomicArgs a{};
         a.nrows = A->nrows;
@@ -564,7 +575,8 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
         a.chp = A->chp.as<uint32_t>();
         a.klen = A->k1len.as<uint32_t>();
         a.col = A->col.as<uint32_t>();
-        a.vidx = vbar_order == GS_VALUES_SLOTS ? A->ftslot.as<uint32_t>() : A->fsrc.as<uint32_t>();
+        // vbar in forward slot order first (coalesced), then gathered into the asked order
+        const bool via_slots = d_vbar != nullptr;
         a.unit_chunk = A->k1unit_chunk.as<uint32_t>();
         a.unit_base = A->k1unit_base.as<uint32_t>();
         a.units = A->k1units;
@@ -572,8 +584,21 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
         a.x = d_X;
         a.ybar = d_Ybar;
         a.xbar = d_Xbar;
-        a.vbar = d_vbar;
-        return f64 ? launch_atomic<double>(a, k, s) : launch_atomic<float>(a, k, s);
+        a.vbar = via_slots ? A->vslots.p : d_vbar;
+        GS_TRY((f64 ? launch_atomic<double>(a, k, s) : launch_atomic<float>(a, k, s)));
+        if (via_slots) {
+            const bool csr = vbar_order == GS_VALUES_CSR;
+            const size_t n_out = csr ? A->nnz : A->tlenVC;
+            const uint32_t *map = csr ? A->csr2f.as<uint32_t>() : A->t2f.as<uint32_t>();
+            if (f64)
+                k_gather_vals<double><<<gb, 256, 0, s>>>(n_out, map, A->vslots.as<double>(),
+                                                         static_cast<double *>(d_vbar));
+            else
+                k_gather_vals<float><<<gb, 256, 0, s>>>(n_out, map, A->vslots.as<float>(),
+                                                        static_cast<float *>(d_vbar));
+            GS_CHECK_LAUNCH();
+        }
+        return GS_OK;
     }
     if (mode != GS_ADJ_DETERMINISTIC) return fail(GS_ERR_INVALID, "unknown adjoint mode %d", (int)mode);
     MMArgs a{};
@@ -584,12 +609,12 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
     a.klen = A->tlen.as<uint32_t>();
     a.val = A->tval.p;
     a.col = A->trow.as<uint32_t>();
-    a.src = A->tsrc.as<uint32_t>();
     a.xin = d_Ybar;
     a.xrow = d_X;
     a.yout = d_Xbar;
-    a.vbar = d_vbar;
-    a.vbar_slots = vbar_order == GS_VALUES_SLOTS;
+    // CSR order: vbar in the adjoint layout's slot order first, then gathered into CSR order
+    const bool via_slots = d_vbar && vbar_order == GS_VALUES_CSR;
+    a.vbar = via_slots ? A->vslots.p : d_vbar;
     a.unit_chunk = A->tunit_chunk.as<uint32_t>();
     a.unit_base = A->tunit_base.as<uint32_t>();
     a.units = A->tunits;
@@ -598,7 +623,19 @@ gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, voi
     a.count = A->tcount.as<uint32_t>();
     a.ld = k;
     a.nrb = 1;
-    return f64 ? launch_mm<double, true>(a, k, s) : launch_mm<float, true>(a, k, s);
+    GS_TRY((f64 ? launch_mm<double, true>(a, k, s) : launch_mm<float, true>(a, k, s)));
+    if (via_slots) {
+        if (f64)
+            k_gather_vals<double><<<gb, 256, 0, s>>>(A->nnz, A->csr2t.as<uint32_t>(),
+                                                     A->vslots.as<double>(),
+                                                     static_cast<double *>(d_vbar));
+        else
+            k_gather_vals<float><<<gb, 256, 0, s>>>(A->nnz, A->csr2t.as<uint32_t>(),
+                                                    A->vslots.as<float>(),
+                                                    static_cast<float *>(d_vbar));
+        GS_CHECK_LAUNCH();
+    }
+    return GS_OK;
 }
 
 }  // extern "C"

@@ -202,8 +202,6 @@ class Matrix:
             return Xb[:, 0], vb
         k = Ybar.shape[1]
         m = L.GS_ADJ_ATOMIC if mode == "atomic" else L.GS_ADJ_DETERMINISTIC
-        if m == L.GS_ADJ_ATOMIC:
-            want_vbar = True
         if want_vbar and X is None:
             raise TypeError("vbar needs X")
         Xbar = torch.empty(self.ncols, k, dtype=dt, device=Ybar.device)

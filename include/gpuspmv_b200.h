@@ -398,8 +398,10 @@ gs_status gs_matrix_convert_values(const gs_matrix *A, const void *d_in,
                                    gs_stream stream);
 /* Xbar = A^T Ybar (Xbar [ncols][k], overwritten) and, when d_vbar is given,
  * vbar[e] = sum_r Ybar[row_e][r] * X[col_e][r] for every stored element e, in vbar_order
- * (the gradient with respect to the values).  The atomic mode needs X and vbar.  X, Ybar
- * and Xbar are 32-byte aligned. */
+ * (the gradient with respect to the values; d_X is then required).  X, Ybar and Xbar are
+ * 32-byte aligned.  A CSR-order vbar is formed in slot order in a buffer of the matrix and
+ * gathered into CSR order (coalesced writes), so calls on one matrix must not overlap.
+ * The atomic mode without d_vbar reads neither X nor a second copy of the values. */
 gs_status gs_spmm_adjoint(gs_matrix *A, const void *d_Ybar, const void *d_X, void *d_Xbar,
                           void *d_vbar, gs_dtype dtype, UIN k, gs_adjoint_mode mode,
                           gs_value_order vbar_order, gs_stream stream);

@@ -84,6 +84,8 @@ def test_adjoint_against_explicit_transpose(port, name, k):
     assert torch.equal(Xbar, Xbar2) and torch.equal(vbar, vbar2)  # reproducible
     Xa, va = A.adjoint(Ybar, X, mode="atomic")
     assert torch.equal(va, vbar)  # same products, same order per element
+    Xa0, va0 = A.adjoint(Ybar, None, mode="atomic", want_vbar=False)  # Xbar only
+    assert va0 is None
     # slot order: the same numbers, in place; padding slots zero
     Xs, vs = A.adjoint(Ybar, X, mode="deterministic", order="slots")
     assert torch.equal(Xs, Xbar) and torch.equal(A.convert_values(vs, to="csr"), vbar)
@@ -92,7 +94,7 @@ def test_adjoint_against_explicit_transpose(port, name, k):
     real = A.convert_values(torch.ones(A.nnz, dtype=torch.float64, device="cuda"), to="slots")
     assert torch.all(vs[real == 0] == 0) and int(real.sum()) == A.nnz
     rowT, colT, valT, _ = _transpose(row, col, val, ncols)
-    Xbar, Xa = Xbar.cpu().numpy(), Xa.cpu().numpy()
+    Xbar, Xa, Xa0 = Xbar.cpu().numpy(), Xa.cpu().numpy(), Xa0.cpu().numpy()
     for r in range(k):
         ref = port.csr_spmv(rowT, colT, valT, Yb[:, r])
         _, mag = port.csr_truth(rowT, colT, valT, Yb[:, r])
@@ -100,6 +102,7 @@ def test_adjoint_against_explicit_transpose(port, name, k):
         # atomic adds: any order of the same terms, |error| <= len_j eps (|A^T||Ybar|)_j
         lens = np.diff(rowT).astype(np.float64)
         assert np.all(np.abs(Xa[:, r] - ref) <= (lens + 1) * 2.0 ** -52 * mag + 1e-300), r
+        assert np.all(np.abs(Xa0[:, r] - ref) <= (lens + 1) * 2.0 ** -52 * mag + 1e-300), r
     rows = np.repeat(np.arange(n), np.diff(row))
     vref = np.einsum("ek,ek->e", Yb[rows], Xh[col])
     vmag = np.einsum("ek,ek->e", np.abs(Yb[rows]), np.abs(Xh[col]))
