@@ -66,6 +66,12 @@ VARIANTS = {
     "axt-unc-th2": dict(fmt="AXT", mode="UNC", tileH=2, tileHW=32),
     "axt-unc-th4": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
     "axt-unc-th8": dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
+    # the first generation's brick formats with x gathered at run time: AXCv0 = AXC with
+    # half-bricks of 16, AXCv1 = AXT UNC tileH 1 tileHW 16, AXBv0 = AXT COM tileH 1 tileHW 16
+    # with a header every 32 positions
+    "axcv0": dict(fmt="AXC", hbs=16),
+    "axcv1": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=16),
+    "axbv0": dict(fmt="AXT", mode="COM", tileH=1, tileHW=16, bs=32),
     # kernel variants of the same layouts (comparison / tuning)
     "axt-com-th8-tma": dict(fmt="AXT", mode="COM", tileH=8, tileHW=32, bs=256, tma=True),
     "axt-unc-th4-tma": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32, tma=True),
@@ -110,7 +116,8 @@ def variant_bytes(n: int, nnz: int, kw: dict, run: dict) -> float:
     return E.algorithmic_bytes(n, n, nnz, 1, s_v, s_i, s_x, s_y)
 DEFAULT_VARIANT = "k1"
 # formats timed beside the headline (µs per product), same matrix and x
-COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc")
+COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc",
+           "axcv0", "axcv1", "axbv0")
 
 
 def make_matrix(workload: str, rank: int, matgen=None):
@@ -464,16 +471,16 @@ def time_batched(steps: int, count: int = 256):
     B.make_operands([matgen.batch_rhs(i, A.ncols, k, seed=3) for i, (A, k) in
                      enumerate(zip(mats, ks))])
     tune = autotune.tune(B, reps=5)
+    tuned = tune["config"]
     us = _time_us(lambda: B.run(graph=True), steps, warm=3)
-    us_default = None
-    kb_tuned = list(B.blocking)
-    B.set_blocking(B.kpad)
-    us_default = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
-    B.set_blocking(kb_tuned)
     paths = B.paths
-    B.set_paths(["k1"] * nm)  # every matrix on K1 units (gathers through L1 / L2)
-    us_k1 = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
-    B.set_paths(["auto"] * nm)
+    row_blocks = B.row_blocks
+    # untuned: every matrix at its full width, the default path and 4096-row blocks
+    autotune.apply_config(B, {"kb": list(B.kpad), "path": ["auto"] * nm, "rows": [4096] * nm})
+    us_default = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)
+    autotune.apply_config(B, {"kb": tuned["kb"], "path": ["k1"] * nm, "rows": tuned["rows"]})
+    us_k1 = _time_us(lambda: B.run(graph=True), max(5, steps // 4), warm=2)  # K1 units only
+    autotune.apply_config(B, tuned)
     # error of every matrix's FP32 result against the FP64 product of the same FP32 values and
     # right-hand sides (torch's sparse CSR product, outside this engine), per row over
     # (|A||X|)_i: the largest over all matrices and columns
@@ -503,7 +510,8 @@ def time_batched(steps: int, count: int = 256):
            "error_vs_fp64": err,
            "error_note": "max over all matrices, rows and columns of |Y - Y64| / (|A||X|)_i, "
                          "Y64 = torch sparse CSR FP64 product of the same FP32 numbers",
-           "autotune": {k: int(v) for k, v in tune["choices"].items()},
+           "autotune": tune["choices"],
+           "row_blocks": sum(b for _, b in row_blocks),
            "autotune_ms": {k: round(v, 3) for k, v in tune["timings"].items()}}
     B.close()
     for A in mats:

@@ -72,6 +72,46 @@ class StrMatAXT(C.Structure):  # cudaSpmv.cu:1154
 
 
 # ------------------------------------------------------------------ second API generation
+class Gen0MatCSR(C.Structure):  # spmv_header.h:247
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("rmin", UIN), ("rave", FPT), ("rmax", UIN),
+                ("rsd", FPT), ("bw", UIN), ("val", FPTp), ("row", UINp), ("col", UINp),
+                ("rl", UINp)]
+
+
+class Gen0FormatData(C.Structure):  # spmv_header.h:370
+    _fields_ = [("name", C.c_char * 12), ("mfp", C.c_double), ("beta", C.c_double),
+                ("ct", C.c_double)]
+
+
+class Gen0Err(C.Structure):  # spmv_header.h:435
+    _fields_ = [("aErr", C.c_double), ("rErr", C.c_double), ("pos", UIN)]
+
+
+class Gen0Res(C.Structure):  # spmv_header.h:464
+    _fields_ = [("name", C.c_char * 24), ("et", C.c_double), ("flops", C.c_double),
+                ("sErr", Gen0Err)]
+
+
+class Gen0MatAXCv0(C.Structure):  # spmv_header.h:665
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("lenAX", UIN), ("lenBRP", UIN), ("ax", FPTp),
+                ("brp", UINp)]
+
+
+class Gen0MatAXCv1(C.Structure):  # spmv_header.h:851
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("lenAX", UIN), ("lenBRP", UIN), ("lenRWP", UIN),
+                ("ax", FPTp), ("brp", UINp), ("rwp", UINp)]
+
+
+class Gen0MatAXBv0(C.Structure):  # spmv_header.h:1649
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("brickNum", UIN), ("lenAX", UIN),
+                ("lenHDR", UIN), ("ax", FPTp), ("hdr0", UINp)]
+
+
+class Gen0MatAXBv1(C.Structure):  # spmv_header.h:2299
+    _fields_ = [("nrows", UIN), ("nnz", UIN), ("brickNum", UIN), ("lenAX", UIN),
+                ("lenHDR", UIN), ("blockLog", UIN), ("ax", FPTp), ("hdr1", UINp)]
+
+
 class Gen2MatCSR(C.Structure):  # gpuSpmv_header.h:252
     _fields_ = [("nrows", UIN), ("nnz", UIN), ("rmin", UIN), ("rave", FPT), ("rmax", UIN),
                 ("rsd", FPT), ("bw", UIN), ("val", FPTp), ("row", UINp), ("col", UINp),
@@ -178,6 +218,21 @@ SIGNATURES = {
     "gs_matrix_destroy": (_st, [_vp]),
     "gs_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
     "gs_dropin_last_y": (UIN, [FPTp, UIN]),
+    "gs0_getFormatDataAXCv0": (Gen0FormatData, [UIN, Gen0MatCSR, FPTp, C.POINTER(Gen0MatAXCv0)]),
+    "gs0_getFormatDataAXCv1": (Gen0FormatData, [UIN, Gen0MatCSR, FPTp, C.POINTER(Gen0MatAXCv1)]),
+    "gs0_getFormatDataAXBv0": (Gen0FormatData, [Gen0MatCSR, FPTp, C.POINTER(Gen0MatAXBv0)]),
+    "gs0_getFormatDataAXBv1": (Gen0FormatData, [UIN, Gen0MatCSR, FPTp, C.POINTER(Gen0MatAXBv1)]),
+    "gs0_testGpuSpmvAXCv0": (Gen0Res, [UIN, Gen0MatAXCv0, FPTp]),
+    "gs0_testGpuSpmvAXCv1_0": (Gen0Res, [UIN, Gen0MatAXCv1, FPTp]),
+    "gs0_testGpuSpmvAXCv1_1": (Gen0Res, [UIN, Gen0MatAXCv1, FPTp]),
+    "gs0_testGpuSpmvAXCv1_2": (Gen0Res, [UIN, Gen0MatAXCv1, FPTp]),
+    "gs0_testGpuSpmvAXCv1_3": (Gen0Res, [UIN, Gen0MatAXCv1, FPTp]),
+    "gs0_testGpuSpmvAXCv1_4": (Gen0Res, [UIN, Gen0MatAXCv1, FPTp]),
+    "gs0_testGpuSpmvAXBv0_0": (Gen0Res, [UIN, Gen0MatAXBv0, FPTp]),
+    "gs0_testGpuSpmvAXBv0_1": (Gen0Res, [UIN, Gen0MatAXBv0, FPTp]),
+    "gs0_testGpuSpmvAXBv0_2": (Gen0Res, [UIN, Gen0MatAXBv0, FPTp]),
+    "gs0_testGpuSpmvAXBv0_3": (Gen0Res, [UIN, Gen0MatAXBv0, FPTp]),
+    "gs0_testGpuSpmvAXBv1_0": (Gen0Res, [UIN, Gen0MatAXBv1, FPTp]),
     "gs_algorithmic_bytes": (C.c_double, [UIN, UIN, UIN, UIN, UIN, UIN, UIN, UIN]),
     "gs_spmv": (_st, [_vp, _vp, C.c_int, _vp, C.c_int, UIN, _vp]),
     "gs_spmv_host": (_st, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.c_int, UIN, _vp]),
@@ -198,6 +253,8 @@ SIGNATURES = {
     "gs_batch_set_blocking": (_st, [_vp, C.POINTER(UIN), _vp]),
     "gs_batch_set_paths": (_st, [_vp, C.POINTER(UIN), _vp]),
     "gs_batch_paths": (_st, [_vp, C.POINTER(UIN)]),
+    "gs_batch_set_row_blocks": (_st, [_vp, C.POINTER(UIN), _vp]),
+    "gs_batch_row_blocks": (_st, [_vp, C.POINTER(UIN), C.POINTER(UIN)]),
     "gs_batch_status": (_st, [_vp, C.POINTER(UIN), _vp]),
     "gs_batch_run": (_st, [_vp, _vp]),
     "gs_batch_run_graph": (_st, [_vp, _vp]),

@@ -1,19 +1,30 @@
-"""Autotuners: the layout of a single matrix (choose_format), and each matrix's
-right-hand-side block width in a batched multi-RHS product (tune).
+"""Autotuners: the layout of a single matrix (choose_format), and the launch shape of each
+matrix in a batched multi-RHS product (tune).
 
-A matrix with kpad right-hand sides runs as kpad/kb passes of kb columns.  Wide blocks
-gather each stored element's x row once for all columns; narrow ones re-read the value and
-column streams per pass but need fewer registers.  The batch kernel is instantiated for its
-widest block, so one wide matrix sets the register budget, and hence the occupancy, of the
-whole launch.  The tuner therefore times whole-batch runs (CUDA events, median of `reps`
-after warm-up):
+A batched matrix has three knobs, the batched counterparts of the reference's sweep over
+tileHeight, threads (warps) per row and block size (cudaSpmv.cu:2349-2417):
+
+  * the right-hand-side block width kb: kpad/kb passes of kb columns.  Wide blocks gather
+    each stored element's X row once for all columns; narrow ones re-read the value and
+    column streams per pass but need fewer registers.  On row blocks kb also sets the lanes
+    per row (16 bytes of the row's kb values per lane: 8 lanes at kb = 32 in FP32);
+  * the path: K1 units (a warp per 32-row unit, X gathered through L1 / L2) or row blocks
+    (a thread block per block of rows, X band staged in shared memory);
+  * the row-block height (rows per block, 32..4096): smaller blocks make more, smaller work
+    items for the persistent kernel to balance.
+
+The batch kernels are instantiated for the widest block, so one wide matrix sets the
+register budget, and hence the occupancy, of the whole launch.  The tuner therefore times
+whole-batch runs (CUDA events, median of `reps` after warm-up):
 
   1. a global cap C in (32, 16, 8, 4): kb_i = min(kpad_i, C);
-  2. one pass over the groups of matrices with the same (kpad, row-length class), trying
-     half the group's width and keeping it when the batch gets faster by more than 1 %.
+  2. one pass over the groups of matrices with the same (kpad, row-length class, size
+     class), trying for each group half its width, the other path, and row-block heights
+     of 1024 and 256, keeping a change when the batch gets faster by more than 1 %.
 
-The choice is stored per group key "<dtype>/kpad<k>/len<class>" in an optional JSON cache,
-which later batches apply without timing.
+The choices are stored per group key "<dtype>/kpad<k>/len<class>/n<class>" in an optional
+JSON cache, which later batches apply without timing.  None of the knobs changes the sums or
+their order: every choice gives the same bits.
 """
 from __future__ import annotations
 
@@ -31,6 +42,10 @@ def _len_class(A) -> int:
     return 0 if avg < 16 else (1 if avg < 48 else 2)
 
 
+def _size_class(A) -> int:
+    return 0 if A.nrows < 20000 else (1 if A.nrows < 100000 else 2)
+
+
 def _time_batch(B: E.Batch, reps: int) -> float:
     for _ in range(2):
         B.run(graph=False)
@@ -45,54 +60,100 @@ def _time_batch(B: E.Batch, reps: int) -> float:
     return statistics.median(ts)
 
 
+class _Config:
+    """kb, requested path and row-block height of every matrix of a batch."""
+
+    def __init__(self, kb, path, rows):
+        self.kb, self.path, self.rows = list(kb), list(path), list(rows)
+
+    def copy(self):
+        return _Config(self.kb, self.path, self.rows)
+
+    def apply(self, batch: E.Batch) -> bool:
+        """Set it on the batch; False (batch unchanged) when a matrix cannot take it."""
+        from . import _lib as L
+
+        try:
+            batch.set_row_blocks(self.rows)
+            batch.set_paths(self.path)
+            batch.set_blocking(self.kb)
+        except L.GSError as e:
+            if e.status != L.GS_ERR_UNSUPPORTED:
+                raise
+            return False
+        return True
+
+
 def tune(batch: E.Batch, reps: int = 5, cache_path: str | None = None) -> dict:
-    """Choose and apply a block width per matrix of `batch` (operands must be set).
-    Returns {"choices": {group key: kb}, "timings": {candidate: ms}}."""
+    """Choose and apply each matrix's right-hand-side block width, path and row-block height
+    (operands must be set).  Returns {"choices": {group key: {"kb", "path", "rows"}},
+    "timings": {candidate: ms}, "untuned_ms", "tuned_ms"}."""
     cache = {}
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
             cache = json.load(f)
     dt = "f64" if batch.dtype == torch.float64 else "f32"
-    keys = [f"{dt}/kpad{kp}/len{_len_class(A)}" for A, kp in zip(batch.mats, batch.kpad)]
+    keys = [f"{dt}/kpad{kp}/len{_len_class(A)}/n{_size_class(A)}"
+            for A, kp in zip(batch.mats, batch.kpad)]
     groups: dict[str, list[int]] = {}
     for i, key in enumerate(keys):
         groups.setdefault(key, []).append(i)
-    if all(k in cache for k in groups):
-        choices = {k: int(cache[k]) for k in groups}
-        batch.set_blocking([choices[k] for k in keys])
-        return {"choices": choices, "timings": {}}
+    n = len(batch.mats)
+    if all(isinstance(cache.get(k), dict) for k in groups):
+        cfg = _Config([cache[k]["kb"] for k in keys], [cache[k]["path"] for k in keys],
+                      [cache[k]["rows"] for k in keys])
+        if cfg.apply(batch):
+            return {"choices": {k: cache[k] for k in groups}, "timings": {},
+                    "config": {"kb": cfg.kb, "path": cfg.path, "rows": cfg.rows}}
 
     timings = {}
-    best_kb, best_t = None, float("inf")
-    for cap in (32, 16, 8, 4):
-        kb = [min(kp, cap) for kp in batch.kpad]
-        if kb == best_kb:
+    base = _Config(batch.kpad, ["auto"] * n, [4096] * n)
+    base.apply(batch)
+    untuned = _time_batch(batch, reps)
+    timings["untuned"] = untuned
+    best, best_t = base, untuned
+    for cap in (16, 8, 4):
+        cfg = best.copy()
+        cfg.kb = [min(kp, cap) for kp in batch.kpad]
+        if cfg.kb == best.kb or not cfg.apply(batch):
             continue
-        batch.set_blocking(kb)
         t = _time_batch(batch, reps)
         timings[f"cap{cap}"] = t
-        if t < best_t:
-            best_kb, best_t = kb, t
-    kb = list(best_kb)
-    for key, idx in groups.items():
-        w = kb[idx[0]]
-        if w == 1 or w * 8 < batch.kpad[idx[0]] * 2:
-            continue
-        trial = list(kb)
-        for i in idx:
-            trial[i] = w // 2
-        batch.set_blocking(trial)
-        t = _time_batch(batch, reps)
-        timings[f"{key}:kb{w // 2}"] = t
         if t < 0.99 * best_t:
-            kb, best_t = trial, t
-    batch.set_blocking(kb)
-    choices = {key: kb[idx[0]] for key, idx in groups.items()}
+            best, best_t = cfg, t
+    for key, idx in groups.items():
+        trials = []
+        w = best.kb[idx[0]]
+        if w > 1:
+            trials.append(("kb%d" % (w // 2), "kb", w // 2))
+        trials.append(("k1" if best.path[idx[0]] != "k1" else "band", "path",
+                       "k1" if best.path[idx[0]] != "k1" else "auto"))
+        for rows in (1024, 256):
+            trials.append(("rows%d" % rows, "rows", rows))
+        for name, knob, value in trials:
+            cfg = best.copy()
+            for i in idx:
+                getattr(cfg, knob)[i] = value
+            if not cfg.apply(batch):
+                continue
+            t = _time_batch(batch, reps)
+            timings[f"{key}:{name}"] = t
+            if t < 0.99 * best_t:
+                best, best_t = cfg, t
+    best.apply(batch)
+    choices = {key: {"kb": best.kb[idx[0]], "path": best.path[idx[0]],
+                     "rows": best.rows[idx[0]]} for key, idx in groups.items()}
     if cache_path:
         cache.update(choices)
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
-    return {"choices": choices, "timings": timings}
+    return {"choices": choices, "timings": timings, "untuned_ms": untuned, "tuned_ms": best_t,
+            "config": {"kb": best.kb, "path": best.path, "rows": best.rows}}
+
+
+def apply_config(batch: E.Batch, config: dict) -> bool:
+    """Set a configuration returned by tune() ({"kb", "path", "rows"} lists) on a batch."""
+    return _Config(config["kb"], config["path"], config["rows"]).apply(batch)
 
 
 # ----------------------------------------------------------------------------- formats

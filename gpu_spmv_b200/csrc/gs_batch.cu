@@ -46,6 +46,7 @@ struct BandBlock {
 // the block | (row - row0) << 16, y = its length.
 struct BandMat {
     bool tried = false, fits = false;
+    uint32_t rows_max = 0;  // rows per block at most (the height of the row blocks)
     DevBuf info, col, val, blocks;
     std::vector<BandBlock> hblocks;
 };
@@ -581,7 +582,7 @@ gs_status build_band_t(gs_batch *B, size_t i, cudaStream_t s)
             const bool empty = lo[r] >= hi[r];
             uint32_t nl = empty ? l : std::min(l, lo[r]), nh = empty ? h : std::max(h, hi[r]);
             uint64_t ne = e + padded(rl[r]);
-            if (r > r0 && (r - r0 >= kBandRowsMax || !fits(nl, nh, ne, r0, r + 1))) {
+            if (r > r0 && (r - r0 >= bm.rows_max || !fits(nl, nh, ne, r0, r + 1))) {
                 blocks.push_back({r0, r, l < h ? l : 0u, l < h ? h : 0u, (uint32_t)etot,
                                   (uint32_t)(etot + e), 0u, 0u});
                 etot += e;
@@ -827,6 +828,7 @@ gs_status gs_batch_create(gs_batch **out, UIN count, gs_matrix *const *mats, con
     B->desc.resize(count);
     B->bdesc.resize(count);
     B->band.resize(count);
+    for (UIN i = 0; i < count; i++) B->band[i].rows_max = kBandRowsMax;
     B->path_req.assign(count, GS_BATCH_AUTO);
     B->path.assign(count, GS_BATCH_K1);
     B->nmc.resize(count);
@@ -943,6 +945,46 @@ gs_status gs_batch_set_blocking(gs_batch *B, const UIN *kb, gs_stream stream)
         build_items(B, cs(stream));
     }
     return st;
+}
+
+gs_status gs_batch_set_row_blocks(gs_batch *B, const UIN *rows_max, gs_stream stream)
+{
+    if (!B || (!B->mats.empty() && !rows_max)) return fail(GS_ERR_INVALID, "NULL argument");
+    for (size_t i = 0; i < B->mats.size(); i++)
+        if (rows_max[i] < 32 || rows_max[i] > kBandRowsMax)
+            return fail(GS_ERR_INVALID, "matrix %zu: %u rows per block (32..%u)", i, rows_max[i],
+                        kBandRowsMax);
+    B->drop_graph();  // it may name the row-block arrays replaced below
+    std::vector<uint32_t> old(B->mats.size());
+    for (size_t i = 0; i < B->mats.size(); i++) {
+        BandMat &bm = B->band[i];
+        old[i] = bm.rows_max;
+        if (bm.rows_max != rows_max[i]) {  // planned again on its next use
+            bm = BandMat();
+            bm.rows_max = rows_max[i];
+        }
+    }
+    const gs_status st = build_items(B, cs(stream));
+    if (st != GS_OK) {
+        for (size_t i = 0; i < B->mats.size(); i++) {
+            if (B->band[i].rows_max != old[i]) {
+                B->band[i] = BandMat();
+                B->band[i].rows_max = old[i];
+            }
+        }
+        build_items(B, cs(stream));
+    }
+    return st;
+}
+
+gs_status gs_batch_row_blocks(const gs_batch *B, UIN *rows_max, UIN *blocks)
+{
+    if (!B) return fail(GS_ERR_INVALID, "NULL argument");
+    for (size_t i = 0; i < B->mats.size(); i++) {
+        if (rows_max) rows_max[i] = B->band[i].rows_max;
+        if (blocks) blocks[i] = B->path[i] == GS_BATCH_BAND ? (UIN)B->band[i].hblocks.size() : 0u;
+    }
+    return GS_OK;
 }
 
 gs_status gs_batch_set_paths(gs_batch *B, const UIN *path, gs_stream stream)

@@ -1098,3 +1098,321 @@ gs2_res gs2_test_gk_AXT_COM_H1(const UIN cudaBlockSize, const gs2_matAXT a, cons
 }
 
 }  // extern "C"
+
+// ======================================================================================
+// First API generation (spmv_header.h), its brick formats AXCv0, AXCv1, AXBv0 and AXBv1,
+// exported as gs0_* (gpuspmv_b200_gen0.h).  Each is a layout the later generation's
+// converters already build, with bricks of 16: AXCv0 = AXC hbs 16 (spmv_header.h:665-760),
+// AXCv1 = AXT UNC tileH 1 tileHW 16 (brp = con, rwp = sec; :851-960), AXBv0 = AXT COM tileH 1
+// tileHW 16 with a header word every 32 positions (hdr0 = sec; :1649-1727), AXBv1 = the same
+// every cudaBlockSize positions with hdr1 padded to a multiple of 32 words (:2299-2390).
+// ======================================================================================
+#define GS0_NO_ALIASES
+#include "gpuspmv_b200_gen0.h"
+
+namespace {
+
+constexpr UIN kGen0Brick = 16;  // HBRICK_SIZE of spmv_header.h (spmv_header.h:97-99)
+
+str_matCSR gen1_view0(const gs0_matCSR &m)
+{
+    str_matCSR v;
+    memset(&v, 0, sizeof(v));
+    strcpy(v.name, "gen0");
+    v.nrows = m.nrows;
+    v.nnz = m.nnz;
+    v.rmin = m.rmin;
+    v.rave = m.rave;
+    v.rmax = m.rmax;
+    v.rsd = m.rsd;
+    v.bw = m.bw;
+    v.val = m.val;
+    v.row = m.row;
+    v.col = m.col;
+    v.rl = m.rl;
+    return v;
+}
+
+gs0_formatData gen0_fd(const char *name, double mfp, double beta, double ct)
+{
+    gs0_formatData fd;
+    memset(&fd, 0, sizeof(fd));
+    snprintf(fd.name, sizeof(fd.name), "%s", name);
+    fd.mfp = mfp;
+    fd.beta = beta;
+    fd.ct = ct;
+    return fd;
+}
+
+gs0_formatData gen0_error_fd()
+{
+    return gen0_fd("error", 0.0, 0.0, 0.0);
+}
+
+gs0_res gen0_res(const str_res &r, const char *name)
+{
+    gs0_res o;
+    memset(&o, 0, sizeof(o));
+    snprintf(o.name, sizeof(o.name), "%s", strcmp(r.name, "error") ? name : "error");
+    o.et = r.et;
+    o.flops = r.flops;
+    o.sErr.aErr = r.sErr.aErr;
+    o.sErr.rErr = r.sErr.rErr;
+    o.sErr.pos = r.sErr.pos;
+    return o;
+}
+
+// UNC tileH 1 tileHW 16 or COM tileH 1 tileHW 16 (header block bs) of a first-generation
+// CSR, through the later generation's converter
+str_formatData gen0_axt(const gs0_matCSR &m, const FPT *vec, const char *mode, UIN bs,
+                        str_matAXT *t)
+{
+    memset(t, 0, sizeof(*t));
+    return getFormatDataAXT(1, bs, kGen0Brick, 1, mode, gen1_view0(m), vec, t);
+}
+
+// first-generation views of the brick formats as later-generation structs, for the products
+str_matAXC axc_view(const gs0_matAXCv0 &a)
+{
+    str_matAXC v;
+    memset(&v, 0, sizeof(v));
+    v.nrows = a.nrows;
+    v.nnz = a.nnz;
+    v.hbs = kGen0Brick;
+    v.lenAX = a.lenAX;
+    v.lenBRP = a.lenBRP;
+    v.ax = a.ax;
+    v.brp = a.brp;
+    return v;
+}
+
+str_matAXT unc_view(const gs0_matAXCv1 &a)
+{
+    str_matAXT v;
+    memset(&v, 0, sizeof(v));
+    strcpy(v.name, "gen0");
+    v.nrows = a.nrows;
+    v.nnz = a.nnz;
+    strcpy(v.mode, "UNC");
+    v.tileHW = kGen0Brick;
+    v.tileH = 1;
+    v.tileN = a.lenRWP;
+    v.lenAX = a.lenAX;
+    v.lenSEC = a.lenRWP;
+    v.lenCON = a.nrows;
+    v.ax = a.ax;
+    v.sec = a.rwp;
+    v.con = a.brp;  // nrows + 1 entries
+    return v;
+}
+
+str_matAXT com_view(UIN nrows, UIN nnz, UIN lenAX, UIN *hdr, UIN lenHDR, UIN log, FPT *ax)
+{
+    str_matAXT v;
+    memset(&v, 0, sizeof(v));
+    strcpy(v.name, "gen0");
+    v.nrows = nrows;
+    v.nnz = nnz;
+    strcpy(v.mode, "COM");
+    v.tileHW = kGen0Brick;
+    v.tileH = 1;
+    v.tileN = lenAX / (2 * kGen0Brick);
+    v.lenAX = lenAX;
+    v.lenSEC = lenHDR;
+    v.log = log;
+    v.bs = 1u << log;
+    v.ax = ax;
+    v.sec = hdr;
+    return v;
+}
+
+gs0_res gen0_error_res(const char *name, const char *what)
+{
+    return gen0_res(error_res(name, what), name);
+}
+
+}  // namespace
+
+extern "C" {
+
+gs0_formatData gs0_getFormatDataAXCv0(const UIN numThreads, const gs0_matCSR m, const FPT *vec,
+                                      gs0_matAXCv0 *a)
+{
+    if (!a) return gen0_error_fd();
+    memset(a, 0, sizeof(*a));
+    str_matAXC a1;
+    memset(&a1, 0, sizeof(a1));
+    const str_formatData fd = getFormatDataAXC(numThreads, kGen0Brick, gen1_view0(m), vec, &a1);
+    if (!strcmp(fd.name, "error")) return gen0_error_fd();
+    free(a1.mapx);
+    a->nrows = a1.nrows;
+    a->nnz = a1.nnz;
+    a->lenAX = a1.lenAX;
+    a->lenBRP = a1.lenBRP;
+    a->ax = a1.ax;
+    a->brp = a1.brp;
+    // spmv_header.h:748-751
+    return gen0_fd("AXCv0", (double)((size_t)a->lenAX * sizeof(FPT)) +
+                               (double)((size_t)a->lenBRP * sizeof(UIN)),
+                   (double)a->nnz / (double)(a->lenAX >> 1), fd.ct);
+}
+
+gs0_formatData gs0_getFormatDataAXCv1(const UIN numThreads, const gs0_matCSR m, const FPT *vec,
+                                      gs0_matAXCv1 *a)
+{
+    (void)numThreads;
+    if (!a) return gen0_error_fd();
+    memset(a, 0, sizeof(*a));
+    str_matAXT t;
+    const str_formatData fd = gen0_axt(m, vec, "UNC", 256, &t);
+    if (!strcmp(fd.name, "error")) return gen0_error_fd();
+    a->nrows = t.nrows;
+    a->nnz = t.nnz;
+    a->lenAX = t.lenAX;
+    a->lenBRP = t.nrows + 1;
+    a->lenRWP = t.lenSEC;
+    a->ax = t.ax;
+    a->brp = t.con;
+    a->rwp = t.sec;
+    // spmv_header.h:965-968
+    return gen0_fd("AXCv1", (double)((size_t)a->lenAX * sizeof(FPT)) +
+                               (double)((size_t)a->lenRWP * sizeof(UIN)),
+                   (double)a->nnz / (double)(a->lenAX >> 1), fd.ct);
+}
+
+gs0_formatData gs0_getFormatDataAXBv0(const gs0_matCSR m, const FPT *vec, gs0_matAXBv0 *a)
+{
+    if (!a) return gen0_error_fd();
+    memset(a, 0, sizeof(*a));
+    str_matAXT t;
+    const str_formatData fd = gen0_axt(m, vec, "COM", 32, &t);
+    if (!strcmp(fd.name, "error")) return gen0_error_fd();
+    free(t.con);
+    a->nrows = t.nrows;
+    a->nnz = t.nnz;
+    a->brickNum = t.tileN;
+    a->lenAX = t.lenAX;
+    a->lenHDR = t.lenSEC;
+    a->ax = t.ax;
+    a->hdr0 = t.sec;
+    // spmv_header.h:1718-1721
+    return gen0_fd("AXBv0", (double)((size_t)a->lenAX * sizeof(FPT)) +
+                               (double)((size_t)a->lenHDR * sizeof(UIN)),
+                   (double)a->nnz / (double)(a->lenAX >> 1), fd.ct);
+}
+
+gs0_formatData gs0_getFormatDataAXBv1(const UIN cudaBlockSize, const gs0_matCSR m,
+                                      const FPT *vec, gs0_matAXBv1 *a)
+{
+    if (!a) return gen0_error_fd();
+    memset(a, 0, sizeof(*a));
+    UIN log = 0;
+    for (UIN i = 5; i < 11; i++)
+        if ((cudaBlockSize >> i) == 1) log = i;
+    if (log == 0 || cudaBlockSize != (1u << log)) {
+        gs::fail(GS_ERR_UNSUPPORTED, "AXBv1 takes a cudaBlockSize that is a power of two in "
+                                     "32..1024 (got %u)", cudaBlockSize);
+        return gen0_fd("error", 0.0, 0.0, 0.0);
+    }
+    str_matAXT t;
+    const str_formatData fd = gen0_axt(m, vec, "COM", cudaBlockSize, &t);
+    if (!strcmp(fd.name, "error")) return gen0_error_fd();
+    free(t.con);
+    // hdr1: the header words, padded with zeros to a multiple of 32 (spmv_header.h:2350)
+    const size_t len = ((size_t)t.lenAX / 2 + 2 * kGen0Brick - 1) / (2 * kGen0Brick) *
+                       (2 * kGen0Brick);
+    UIN *hdr = static_cast<UIN *>(calloc(len ? len : 1, sizeof(UIN)));
+    if (!hdr) {
+        free(t.ax);
+        free(t.sec);
+        gs::fail(GS_ERR_ALLOC, "AXBv1 header allocation");
+        return gen0_error_fd();
+    }
+    if (t.lenSEC) memcpy(hdr, t.sec, (size_t)t.lenSEC * sizeof(UIN));
+    free(t.sec);
+    a->nrows = t.nrows;
+    a->nnz = t.nnz;
+    a->brickNum = t.tileN;
+    a->lenAX = t.lenAX;
+    a->lenHDR = (UIN)len;
+    a->blockLog = log;
+    a->ax = t.ax;
+    a->hdr1 = hdr;
+    // spmv_header.h:2379-2382
+    return gen0_fd("AXBv1", (double)((size_t)a->lenAX * sizeof(FPT)) +
+                               (double)((size_t)a->lenHDR * sizeof(UIN)),
+                   (double)a->nnz / (double)(a->lenAX >> 1), fd.ct);
+}
+
+gs0_res gs0_testGpuSpmvAXCv0(const UIN cudaBlockSize, const gs0_matAXCv0 a, const FPT *ref)
+{
+    return gen0_res(test_gaxc(cudaBlockSize, axc_view(a), ref), "gk_AXCv0");
+}
+
+static gs0_res axcv1(const char *name, const gs0_matAXCv1 &a, const FPT *ref)
+{
+    if (a.lenBRP != a.nrows + 1) return gen0_error_res(name, "lenBRP must be nrows + 1");
+    return gen0_res(test_gaxtuh1hw16w(0, 0, unc_view(a), ref), name);
+}
+gs0_res gs0_testGpuSpmvAXCv1_0(const UIN c, const gs0_matAXCv1 a, const FPT *r)
+{
+    (void)c;
+    return axcv1("gk_AXCv1_0", a, r);
+}
+gs0_res gs0_testGpuSpmvAXCv1_1(const UIN c, const gs0_matAXCv1 a, const FPT *r)
+{
+    (void)c;
+    return axcv1("gk_AXCv1_1", a, r);
+}
+gs0_res gs0_testGpuSpmvAXCv1_2(const UIN c, const gs0_matAXCv1 a, const FPT *r)
+{
+    (void)c;
+    return axcv1("gk_AXCv1_2", a, r);
+}
+gs0_res gs0_testGpuSpmvAXCv1_3(const UIN c, const gs0_matAXCv1 a, const FPT *r)
+{
+    (void)c;
+    return axcv1("gk_AXCv1_3", a, r);
+}
+gs0_res gs0_testGpuSpmvAXCv1_4(const UIN c, const gs0_matAXCv1 a, const FPT *r)
+{
+    (void)c;
+    return axcv1("gk_AXCv1_4", a, r);
+}
+
+static gs0_res axb(const char *name, UIN nrows, UIN nnz, UIN lenAX, UIN *hdr, UIN lenHDR,
+                   UIN log, FPT *ax, const FPT *ref)
+{
+    if (lenHDR < lenAX / 2) return gen0_error_res(name, "header array shorter than lenAX / 2");
+    return gen0_res(test_gaxtch1(0, com_view(nrows, nnz, lenAX, hdr, lenAX / 2, log, ax), ref),
+                    name);
+}
+gs0_res gs0_testGpuSpmvAXBv0_0(const UIN c, const gs0_matAXBv0 a, const FPT *r)
+{
+    (void)c;
+    return axb("gk_AXBv0_0", a.nrows, a.nnz, a.lenAX, a.hdr0, a.lenHDR, 5, a.ax, r);
+}
+gs0_res gs0_testGpuSpmvAXBv0_1(const UIN c, const gs0_matAXBv0 a, const FPT *r)
+{
+    (void)c;
+    return axb("gk_AXBv0_1", a.nrows, a.nnz, a.lenAX, a.hdr0, a.lenHDR, 5, a.ax, r);
+}
+gs0_res gs0_testGpuSpmvAXBv0_2(const UIN c, const gs0_matAXBv0 a, const FPT *r)
+{
+    (void)c;
+    return axb("gk_AXBv0_2", a.nrows, a.nnz, a.lenAX, a.hdr0, a.lenHDR, 5, a.ax, r);
+}
+gs0_res gs0_testGpuSpmvAXBv0_3(const UIN c, const gs0_matAXBv0 a, const FPT *r)
+{
+    (void)c;
+    return axb("gk_AXBv0_3", a.nrows, a.nnz, a.lenAX, a.hdr0, a.lenHDR, 5, a.ax, r);
+}
+gs0_res gs0_testGpuSpmvAXBv1_0(const UIN c, const gs0_matAXBv1 a, const FPT *r)
+{
+    (void)c;
+    if (a.blockLog < 5 || a.blockLog > 10)
+        return gen0_error_res("gk_AXBv1_0", "blockLog must be 5..10");
+    return axb("gk_AXBv1_0", a.nrows, a.nnz, a.lenAX, a.hdr1, a.lenHDR, a.blockLog, a.ax, r);
+}
+
+}  // extern "C"

@@ -598,7 +598,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 // is exactly one tile and lane l owns its column l: element k of that column is slot
 // w * 32V + 32k + l, with no division by the runtime tile size.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
-          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false>
+          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false, bool EARLY = false>
 __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -630,6 +630,23 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
             if (over && !seen) break;
             const uint32_t qb = w * WS + (uint32_t)lane * V;
             const bool inb = qb < a.npos;  // rows end on V boundaries: whole lanes only
+            // EARLY: the tile's value and column slots (every slot of a tile exists) and the
+            // real bits load together with the start bits, not after them
+            [[maybe_unused]] VT ev[V];
+            [[maybe_unused]] IT ec[V];
+            [[maybe_unused]] uint32_t erb = FULLV;
+            if constexpr (EARLY) {
+                static_assert(TILED && T32, "early loads are for 32-wide tiles");
+                const uint32_t s0 = w * WS + (uint32_t)lane;
+#pragma unroll
+                for (int k = 0; k < V; k++) {
+                    ev[k] = ld_stream(val + s0 + 32u * (uint32_t)k);
+                    ec[k] = ld_stream(col + s0 + 32u * (uint32_t)k);
+                }
+                // V divides 32 and qb is a multiple of V: the lane's bits sit in one word
+                if constexpr (PADDED)
+                    erb = inb ? ((__ldg(a.rbits + (qb >> 5)) >> (qb & 31)) & FULLV) : 0u;
+            }
             const bool st = inb && ((__ldg(a.sbits + (qb >> 5)) >> (qb & 31)) & 1u);
             const unsigned smask = __ballot_sync(kFull, st);
             unsigned vl = __ballot_sync(kFull, inb);
@@ -643,7 +660,8 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
             }
             const bool valid = (vl >> lane) & 1u;
             uint32_t rb = valid ? FULLV : 0u;
-            if constexpr (PADDED) rb &= get_bits(a.rbits, qb, V);
+            if constexpr (EARLY) rb &= erb;
+            else if constexpr (PADDED) rb &= get_bits(a.rbits, qb, V);
             // ---- the lane's partial sum (loads and gathers of real positions only)
             AT acc = (AT)0;
             if (rb) {
@@ -668,7 +686,13 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                 } else {
                     VT v[V];
                     IT c[V];
-                    if constexpr (TILED) {
+                    if constexpr (EARLY) {
+#pragma unroll
+                        for (int k = 0; k < V; k++) {
+                            v[k] = ev[k];
+                            c[k] = ec[k];
+                        }
+                    } else if constexpr (TILED) {
                         uint32_t s0, stride;
                         if constexpr (T32) {
                             s0 = w * WS + (uint32_t)lane;
@@ -1076,10 +1100,15 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
     uint32_t blocks = min((warps + 7) / 8, 148u * 256u);
     const bool empty = a.n_empty != 0;
     const bool t32 = TILED && a.thw == 32 && a.th == (uint32_t)V;
+    // 32-wide tiles with x gathered at run time load a tile's streams with its start bits,
+    // not after them (power-law UNC th=4 324 -> 320 us, th=8 348 -> 337; 27-point stencil
+    // th=4 334 -> 289, th=8 412 -> 322; the same bits).  The direct layouts keep the
+    // dependent loads: there the early loads cost 8 registers (48 for 8 positions per
+    // lane) and AXC on the power-law went 461 -> 558 us.
 #define GS_L(P, E)                                                                          \
     do {                                                                                    \
         if (t32)                                                                            \
-            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED>            \
+            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED, TILED && !BAKED> \
                 <<<blocks, 256, 0, s>>>(a);                                                 \
         else                                                                                \
             k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, false>            \

@@ -369,6 +369,23 @@ class Batch:
         L.check(L.lib().gs_batch_set_paths(self._h, arr, stream_handle(stream)),
                 "gs_batch_set_paths")
 
+    def set_row_blocks(self, rows_max, stream=None):
+        """Height of each matrix's row blocks (32..4096 rows; the row-block path's
+        tileHeight)."""
+        n = len(self.mats)
+        arr = (L.UIN * max(1, n))(*[int(r) for r in rows_max])
+        L.check(L.lib().gs_batch_set_row_blocks(self._h, arr, stream_handle(stream)),
+                "gs_batch_set_row_blocks")
+
+    @property
+    def row_blocks(self):
+        """(height, number of row blocks) per matrix; 0 blocks for a matrix on K1 units."""
+        n = len(self.mats)
+        h = (L.UIN * max(1, n))()
+        b = (L.UIN * max(1, n))()
+        L.check(L.lib().gs_batch_row_blocks(self._h, h, b), "gs_batch_row_blocks")
+        return [(int(h[i]), int(b[i])) for i in range(n)]
+
     @property
     def paths(self):
         """The path each matrix runs on: "k1" or "band"."""

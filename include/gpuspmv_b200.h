@@ -445,6 +445,16 @@ gs_status gs_batch_set_blocking(gs_batch *B, const UIN *kb, gs_stream stream);
 gs_status gs_batch_set_paths(gs_batch *B, const UIN *path, gs_stream stream);
 /* The path each matrix runs on (GS_BATCH_K1 or GS_BATCH_BAND; array of count). */
 gs_status gs_batch_paths(const gs_batch *B, UIN *path);
+/* Height of each matrix's row blocks: at most rows_max[i] consecutive rows per block
+ * (32..4096, default 4096; a block also ends where its rows and X band would overflow the
+ * shared-memory stage).  The analogue of the reference's tileHeight for the row-block path:
+ * lower heights give more, smaller work items.  Re-plans the changed matrices' blocks and
+ * rebuilds the work list (drops a captured graph); the sums and their order do not depend
+ * on it. */
+gs_status gs_batch_set_row_blocks(gs_batch *B, const UIN *rows_max, gs_stream stream);
+/* Each matrix's row-block height and its number of row blocks (0 when it runs as K1
+ * units); either array may be NULL. */
+gs_status gs_batch_row_blocks(const gs_batch *B, UIN *rows_max, UIN *blocks);
 /* Reads and clears the batch's device status word (synchronises): bit 0 set when a row
  * block's shared-memory copies did not arrive within the bounded wait (its products were
  * not written). */

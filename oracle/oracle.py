@@ -301,6 +301,15 @@ class Ref:
                     l2 = C.CDLL(REF_SPMV_SO)
                     l2.ref_cpuSpmvCSR.restype = None
                     l2.ref_cpuSpmvCSR.argtypes = [u32, u32, _f64p, _u32p, _u32p, _f64p, _f64p]
+                    if hasattr(l2, "ref0_convert"):
+                        PP = C.POINTER
+                        l2.ref0_convert.restype = None
+                        l2.ref0_convert.argtypes = [C.c_int, u32, u32, u32, _f64p, _u32p,
+                                                    _u32p, _f64p, _f64p,
+                                                    PP(PP(C.c_double)), PP(PP(u32)),
+                                                    PP(PP(u32)), _u32p, C.c_char_p]
+                        l2.ref0_free.restype = None
+                        l2.ref0_free.argtypes = [C.c_void_p]
                     Ref._lib_spmv = l2
         self.lib = Ref._lib
         self.lib_spmv = Ref._lib_spmv
@@ -311,6 +320,45 @@ class Ref:
         y = np.empty(n, np.float64)
         self.lib.ref_ncsr(threads or os.cpu_count() or 1, n, int(row[-1]), val, col, row, x, y)
         return y
+
+    GEN0_KINDS = {"AXCv0": 0, "AXCv1": 1, "AXBv0": 2, "AXBv1": 3}
+
+    def gen0(self, kind, row, col, val, x, cbs=256):
+        """A brick format of the first generation (spmv_header.h: getFormatDataAXCv0,
+        AXCv1, AXBv0, AXBv1) as the reference's own converter builds it: dict with ax, the
+        index arrays (brp / rwp / hdr), blockLog (AXBv1), fd (mfp, beta, ct) and name."""
+        row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)
+        n = len(row) - 1
+        fd = np.zeros(3, np.float64)
+        lens = np.zeros(4, np.uint32)
+        name = C.create_string_buffer(16)
+        pax = C.POINTER(C.c_double)()
+        p1 = C.POINTER(C.c_uint32)()
+        p2 = C.POINTER(C.c_uint32)()
+        lib = self.lib_spmv
+        lib.ref0_convert(self.GEN0_KINDS[kind], cbs, n, int(row[-1]), val, col, row, x, fd,
+                         C.byref(pax), C.byref(p1), C.byref(p2), lens, name)
+
+        def take(p, k, dt):
+            if not p or k == 0:
+                out = np.zeros(0, dt)
+            else:
+                out = np.ctypeslib.as_array(p, shape=(int(k),)).copy()
+            if p:
+                lib.ref0_free(C.cast(p, C.c_void_p))
+            return out
+
+        out = dict(ax=take(pax, lens[0], np.float64), fd=fd, name=name.value.decode(),
+                   blockLog=int(lens[3]))
+        i1 = take(p1, lens[1], np.uint32)
+        i2 = take(p2, lens[2], np.uint32)
+        if kind in ("AXCv0", "AXCv1"):
+            out["brp"] = i1
+        if kind == "AXCv1":
+            out["rwp"] = i2
+        if kind in ("AXBv0", "AXBv1"):
+            out["hdr"] = i1
+        return out
 
     def cpu_spmv_csr(self, row, col, val, x):
         row, col, val, x = _u32(row), _u32(col), _f64(val), _f64(x)

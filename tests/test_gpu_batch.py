@@ -244,3 +244,38 @@ def test_row_blocks_edge_matrices(dtype):
         assert torch.all(y[torch.from_numpy(np.diff(r.astype(np.int64)) == 0).cuda()] == 0)
     assert B.status() == 0
     B.close()
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_row_block_height_keeps_bits(dtype):
+    """Lower row-block heights cut the same matrices into more blocks and leave every sum and
+    its order unchanged; out-of-range heights are refused and change nothing."""
+    from gpu_spmv_b200 import GSError
+    from gpu_spmv_b200 import engine as E
+
+    rng = np.random.default_rng(17)
+    mats = _banded_mats(dtype, rng, 6, long_rows=True)
+    ks = [1, 4, 8, 16, 32, 3]
+    B = E.Batch(mats, ks)
+    X, Y = B.make_operands([rng.standard_normal((A.ncols, k)) for A, k in zip(mats, ks)])
+    ref = [A.spmm(x) for A, x in zip(mats, X)]
+    assert [h for h, _ in B.row_blocks] == [4096] * 6
+    blocks0 = [b for _, b in B.row_blocks]
+    for height in (1024, 256, 32):
+        B.set_row_blocks([height] * 6)
+        hb = B.row_blocks
+        assert [h for h, _ in hb] == [height] * 6
+        assert all(b >= b0 for (_, b), b0 in zip(hb, blocks0))
+        for graph in (False, True):
+            for y in Y:
+                y.fill_(float("nan"))
+            B.run(graph=graph)
+            torch.cuda.synchronize()
+            for y, r in zip(Y, ref):
+                assert torch.equal(y, r), height
+    assert sum(b for _, b in B.row_blocks) > sum(blocks0)
+    with pytest.raises(GSError, match="rows per block"):
+        B.set_row_blocks([16] * 6)
+    assert [h for h, _ in B.row_blocks] == [32] * 6
+    assert B.status() == 0
+    B.close()

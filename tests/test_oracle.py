@@ -146,3 +146,38 @@ def test_restatement_equals_reference_at_benchmark_size(port, ref, powerlaw_64m)
         a = port.axt(row, col, val, thw, th, mode, x=x)
         for f in ("ax", "sec", "con"):
             assert np.array_equal(a[f], a_ref[f]), (mode, th, f)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gen0_brick_formats_are_axc_and_axt_layouts(port, ref, name):
+    """The first generation's brick formats (spmv_header.h, compiled unchanged) are layouts
+    the restated converters already build, with bricks of HBRICK_SIZE = 16:
+    AXCv0 = AXC hbs 16 (brp, ax; spmv_header.h:665-760); AXCv1 = AXT UNC tileH 1 tileHW 16
+    (brp = con, rwp = sec; :851-960); AXBv0 = AXT COM tileH 1 tileHW 16 with a header word
+    every 32 positions (hdr0 = sec, bs = 32; :1649-1727); AXBv1 = the same with a header
+    every cudaBlockSize positions, hdr1 padded to a multiple of 32 words (:2299-2390)."""
+    if ref.lib_spmv is None or not hasattr(ref.lib_spmv, "ref0_convert"):
+        pytest.skip("first-generation oracle library not built")
+    rng = np.random.default_rng(sum(map(ord, name)) + 5)
+    row, col, val = case(name, rng)
+    n = len(row) - 1
+    x = rng.uniform(-1, 1, max(n, int(col.max()) + 1))
+    a0 = ref.gen0("AXCv0", row, col, val, x)
+    pa = port.axc(row, col, val, x=x, hbs=16)
+    assert np.array_equal(a0["ax"], pa["ax"]) and np.array_equal(a0["brp"], pa["brp"])
+    a1 = ref.gen0("AXCv1", row, col, val, x)
+    pu = port.axt(row, col, val, 16, 1, "UNC", x=x)
+    assert np.array_equal(a1["ax"], pu["ax"]) and np.array_equal(a1["brp"], pu["con"])
+    assert np.array_equal(a1["rwp"], pu["sec"])
+    b0 = ref.gen0("AXBv0", row, col, val, x)
+    pc = port.axt(row, col, val, 16, 1, "COM", bs=32, x=x)
+    assert np.array_equal(b0["ax"], pc["ax"]) and np.array_equal(b0["hdr"], pc["sec"])
+    for cbs in (64, 256, 1024):
+        b1 = ref.gen0("AXBv1", row, col, val, x, cbs=cbs)
+        pc = port.axt(row, col, val, 16, 1, "COM", bs=cbs, x=x)
+        assert b1["blockLog"] == cbs.bit_length() - 1
+        assert np.array_equal(b1["ax"], pc["ax"])
+        assert len(b1["hdr"]) == (len(pc["sec"]) + 31) // 32 * 32
+        assert np.array_equal(b1["hdr"][:len(pc["sec"])], pc["sec"])
+        assert not b1["hdr"][len(pc["sec"]):].any()
+    assert (a0["name"], a1["name"], b0["name"]) == ("AXCv0", "AXCv1", "AXBv0")
