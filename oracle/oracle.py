@@ -291,6 +291,8 @@ class Ref:
                     "ref_gpu_axc": (C.c_double, [vp, u32, _f64p, _f64p]),
                     "ref_gpu_axt_uh": (C.c_double, [vp, u32, u32, _f64p, _f64p]),
                     "ref_gpu_axt_uh1hw16": (C.c_double, [vp, u32, u32, _f64p, _f64p]),
+                    "ref_gpu_axt_ch1": (C.c_double, [vp, _f64p, _f64p]),
+                    "ref_gpu_axt_ch": (C.c_double, [vp, u32, _f64p, _f64p]),
                 }
                 for name, (res, args) in sig.items():
                     f = getattr(lib, name)
@@ -443,8 +445,9 @@ class Ref:
     # ---- the reference's own GPU products (its kernels compiled for sm_100a; GPU needed)
     def gpu_products(self, row, col, val, x, ref, cbs=256, tpw=4, th=4, reps=5):
         """Device seconds of one launch (median of `reps` calls) of the reference's gcsr,
-        gk1, gaxc (hbs 32), gaxtuh (tileH th, tileHW 32, tpw tiles per warp) and gaxtuh1hw16w
-        (tileH 1, tileHW 16, 128 slots per warp) on this matrix, and each one's get_errors
+        gk1, gaxc (hbs 32), gaxtuh (tileH th, tileHW 32, tpw tiles per warp), gaxtuh1hw16w
+        (tileH 1, tileHW 16, 128 slots per warp), gaxtch1 (COM tileH 1, tileHW 32, header
+        block = cbs) and gaxtch (COM tileH th, tileHW 32) on this matrix, and each one's get_errors
         summary against `ref`.  x is baked into the AXC / AXT layouts, as the reference does.
         The matrix must have no all-empty 32-row chunk (gk1 reads a chunk's first slot
         unconditionally)."""
@@ -474,6 +477,12 @@ class Ref:
         self.lib.ref_axt_free(h)
         h = self.lib.ref_axt(threads, 256, 16, 1, b"UNC", n, nnz, val, col, row, x, fd, None)
         run("gaxtuh1hw16", lambda e: self.lib.ref_gpu_axt_uh1hw16(h, 128, cbs, ref, e))
+        self.lib.ref_axt_free(h)
+        h = self.lib.ref_axt(threads, cbs, 32, 1, b"COM", n, nnz, val, col, row, x, fd, None)
+        run("gaxtch1", lambda e: self.lib.ref_gpu_axt_ch1(h, ref, e))
+        self.lib.ref_axt_free(h)
+        h = self.lib.ref_axt(threads, 256, 32, th, b"COM", n, nnz, val, col, row, x, fd, None)
+        run(f"gaxtch{th}", lambda e: self.lib.ref_gpu_axt_ch(h, cbs, ref, e))
         self.lib.ref_axt_free(h)
         return out
 

@@ -14,8 +14,9 @@
  *   ref_k1_*           -> getFormatDataK1    (cudaSpmv.cu:782-846)
  *   ref_axc_*          -> getFormatDataAXC   (cudaSpmv.cu:1004-1062)
  *   ref_axt_*          -> getFormatDataAXT   (cudaSpmv.cu:1391-1566)
- *   ref_gpu_*          -> test_gcsr, test_gk1, test_gaxc, test_gaxtuh, test_gaxtuh1hw16w
- *                         (the reference's own GPU products, cudaSpmv.cu:547-2037)
+ *   ref_gpu_*          -> test_gcsr, test_gk1, test_gaxc, test_gaxtuh, test_gaxtuh1hw16w,
+ *                         test_gaxtch1, test_gaxtch (the reference's own GPU products,
+ *                         cudaSpmv.cu:547-2285)
  *   ref_struct_layout  -> sizeof / offsetof of the reference's host-API structs
  *
  * No reference code is copied here: the wrappers only marshal arguments into the
@@ -237,6 +238,19 @@ double ref_gpu_axt_uh(void *h, UIN tpw, UIN cbs, const FPT *ref, double *err3)
 double ref_gpu_axt_uh1hw16(void *h, UIN wpw, UIN cbs, const FPT *ref, double *err3)
 {
     return res_out(test_gaxtuh1hw16w(wpw, cbs, *(str_matAXT *)h, ref), err3); /* :1603 */
+}
+
+/* COM tileH = 1: gaxtch1 launched with cudaBlockSize equal to the layout's header block bs
+ * (its segment offset o <= bs - 1 - tid indexes the block's shared array, cudaSpmv.cu:2087) */
+double ref_gpu_axt_ch1(void *h, const FPT *ref, double *err3)
+{
+    const str_matAXT *m = (const str_matAXT *)h;
+    return res_out(test_gaxtch1(m->bs, *m, ref), err3);                  /* cudaSpmv.cu:2101 */
+}
+/* COM tileH > 1, tileHW 32 */
+double ref_gpu_axt_ch(void *h, UIN cbs, const FPT *ref, double *err3)
+{
+    return res_out(test_gaxtch(cbs, *(str_matAXT *)h, ref), err3);        /* cudaSpmv.cu:2213 */
 }
 
 /* sizeof and the offset of every field of the reference's host-API structs, in the order

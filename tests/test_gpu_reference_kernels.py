@@ -1,5 +1,5 @@
-"""The reference's own GPU products (gcsr, gk1, gaxc, gaxtuh, gaxtuh1hw16w from
-cudaSpmv.cu:531-2037, compiled unchanged for sm_100a into oracle/_ref) beside the engine's
+"""The reference's own GPU products (gcsr, gk1, gaxc, gaxtuh, gaxtuh1hw16w, gaxtch1, gaxtch
+from cudaSpmv.cu:531-2285, compiled unchanged for sm_100a into oracle/_ref) beside the engine's
 drop-in entry points of the same names, on the same matrices and x (x baked into the AXC /
 AXT layouts, as the reference's converters do).  Both meet the reference's own error check
 against its CPU ncsr; on the power-law matrix the engine's K1 product takes less device time
@@ -57,11 +57,14 @@ def test_reference_gpu_products_beside_dropin(ref, port, which):
         lib.getFormatDataAXC(1, 32, h.s, R.f64p(x), C.byref(a))
         ours["gaxc"] = lib.test_gaxc(256, a, R.f64p(y_ref))
         R.free_struct_arrays(a, ("ax", "brp", "mapx"))
-        for thw, th, key, fn in ((32, 4, "gaxtuh4", lambda t: lib.test_gaxtuh(4, 256, t, R.f64p(y_ref))),
-                                 (16, 1, "gaxtuh1hw16",
-                                  lambda t: lib.test_gaxtuh1hw16w(128, 256, t, R.f64p(y_ref)))):
+        for mode, thw, th, key, fn in (
+                (b"UNC", 32, 4, "gaxtuh4", lambda t: lib.test_gaxtuh(4, 256, t, R.f64p(y_ref))),
+                (b"UNC", 16, 1, "gaxtuh1hw16",
+                 lambda t: lib.test_gaxtuh1hw16w(128, 256, t, R.f64p(y_ref))),
+                (b"COM", 32, 1, "gaxtch1", lambda t: lib.test_gaxtch1(256, t, R.f64p(y_ref))),
+                (b"COM", 32, 4, "gaxtch4", lambda t: lib.test_gaxtch(256, t, R.f64p(y_ref)))):
             t = L.StrMatAXT()
-            lib.getFormatDataAXT(1, 256, thw, th, b"UNC", h.s, R.f64p(x), C.byref(t))
+            lib.getFormatDataAXT(1, 256, thw, th, mode, h.s, R.f64p(x), C.byref(t))
             ours[key] = fn(t)
             R.free_struct_arrays(t, ("ax", "sec", "con"))
     finally:
