@@ -328,6 +328,25 @@ __device__ __forceinline__ uint32_t baked_index(uint32_t s, uint32_t w)
 
 // Products of the lane's real positions, loaded from global memory (vectorised streaming
 // loads for direct layouts, one coalesced load per tile row for tiled layouts).
+// First slot of a lane's tile column in a tiled layout whose windows hold th positions per
+// lane (V = th): the lane's positions qb = 32 V w + V lane are tile column u = 32 w + lane
+// counted over all tiles, so the tile is u / thw and the column u % thw -- shifts for the
+// power-of-two widths the reference uses, one division otherwise.
+__device__ __forceinline__ uint32_t tile_slot0(const RowsArgs &a, uint32_t w, int lane)
+{
+    const uint32_t u = w * 32u + (uint32_t)lane;
+    uint32_t t, c;
+    if ((a.thw & (a.thw - 1u)) == 0u) {
+        const uint32_t lg = (uint32_t)__ffs(a.thw) - 1u;
+        t = u >> lg;
+        c = u & (a.thw - 1u);
+    } else {
+        t = u / a.thw;
+        c = u - t * a.thw;
+    }
+    return t * a.th * a.thw + c;
+}
+
 template <class VT, class IT, class XT, class PT, int VM, bool TILED, bool BAKED>
 __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint32_t qb,
                                              uint32_t V, uint32_t rb, PT (&prod)[VM])
@@ -336,19 +355,16 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
     const IT *col = static_cast<const IT *>(a.col);
     const XT *x = static_cast<const XT *>(a.x);
     const double *ax = static_cast<const double *>(a.val);
-    const uint32_t ths = a.th * a.thw;
 #pragma unroll
     for (int k = 0; k < VM; k++) prod[k] = (PT)0;
     if (!rb) return;
+    const uint32_t ts0 = TILED ? tile_slot0(a, w, (int)(threadIdx.x & 31u)) : 0u;
     if constexpr (BAKED) {
 #pragma unroll
         for (int k = 0; k < VM; k++) {
             if (k < (int)V && ((rb >> k) & 1u)) {
                 uint32_t s = qb + k;
-                if constexpr (TILED) {
-                    const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
-                    s = t * ths + (uint32_t)k * a.thw + c;
-                }
+                if constexpr (TILED) s = ts0 + (uint32_t)k * a.thw;
                 const uint32_t ai = baked_index(s, a.axw);
                 prod[k] = (PT)mul_rn(__ldcs(ax + ai), __ldcs(ax + ai + a.axw));
             }
@@ -378,8 +394,7 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
         for (int k = 0; k < VM; k++)
             if ((rb >> k) & 1u) prod[k] = mul_rn((PT)ValTraits<VT>::to_f64(v[k]), (PT)xv[k]);
     } else {
-        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
-        const uint32_t s0 = t * ths + cc;
+        const uint32_t s0 = ts0;
         VT v[VM];
         IT c[VM];
 #pragma unroll
@@ -422,7 +437,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
     d.rraw = PADDED ? get_bits(a.rbits, qb, V) : 0xffffffffu;
     const VT *val = static_cast<const VT *>(a.val);
     const IT *col = static_cast<const IT *>(a.col);
-    const uint32_t ths = a.th * a.thw;
+    const uint32_t ts0 = TILED ? tile_slot0(a, w, lane) : 0u;
     if constexpr (BAKED) {
         const double *ax = static_cast<const double *>(a.val);
         if constexpr (!TILED && VM == 8) {
@@ -442,10 +457,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
             d.xb[k] = 0.0;
             if (k < (int)V && qb + k < a.npos) {
                 uint32_t s = qb + k;
-                if constexpr (TILED) {
-                    const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
-                    s = t * ths + (uint32_t)k * a.thw + cc;
-                }
+                if constexpr (TILED) s = ts0 + (uint32_t)k * a.thw;
                 const uint32_t ai = baked_index(s, a.axw);
                 d.v[k] = __ldcs(ax + ai);
                 d.xb[k] = __ldcs(ax + ai + a.axw);
@@ -466,8 +478,7 @@ __device__ __forceinline__ void load_win(const RowsArgs &a, uint32_t w, int lane
             }
         }
     } else {
-        const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
-        const uint32_t s0 = t * ths + cc;
+        const uint32_t s0 = ts0;
 #pragma unroll
         for (int k = 0; k < VM; k++) {
             d.v[k] = (VT)0;
@@ -609,7 +620,6 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
     const double *ax = static_cast<const double *>(a.val);
     constexpr uint32_t WS = 32u * V;
     constexpr uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
-    const uint32_t ths = a.th * a.thw;
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const unsigned mine = 0xffffffffu >> (31 - lane);  // lanes 0..lane
@@ -675,8 +685,7 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                             if constexpr (TILED && T32) {
                                 s = w * WS + 32u * (uint32_t)k + (uint32_t)lane;
                             } else if constexpr (TILED) {
-                                const uint32_t t = qb / ths, c = (qb - t * ths) / a.th;
-                                s = t * ths + (uint32_t)k * a.thw + c;
+                                s = tile_slot0(a, w, lane) + (uint32_t)k * a.thw;
                             }
                             const uint32_t ai = T32 ? (s >> 5) * 64u + (s & 31u)
                                                     : baked_index(s, a.axw);
@@ -698,8 +707,7 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
                             s0 = w * WS + (uint32_t)lane;
                             stride = 32u;
                         } else {
-                            const uint32_t t = qb / ths, cc = (qb - t * ths) / a.th;
-                            s0 = t * ths + cc;
+                            s0 = tile_slot0(a, w, lane);
                             stride = a.thw;
                         }
 #pragma unroll
