@@ -29,7 +29,7 @@
 //   one launch per SpMV.
 // * Staging.  k_rows loads the value/column streams with vectorised streaming loads
 //   (direct layouts: 32 bytes per lane and request when the streams are 32-byte aligned)
-//   or coalesced per-tile-row loads (tiled layouts, tileH <= 4 a window ahead).  k_rows_tma, for the
+//   or coalesced per-tile-row loads (tiled layouts).  k_rows_tma, for the
 //   tiled layouts with 32-wide tiles, streams whole tiles into a per-warp ring of shared
 //   memory stages with 1-D TMA bulk copies (cp.async.bulk, no multicast) completing on
 //   mbarriers, several tiles ahead of the warp; the L1 then serves only the x gathers,
@@ -418,8 +418,7 @@ __device__ __forceinline__ void products_ldg(const RowsArgs &a, uint32_t w, uint
 }
 
 // One window's streams as loaded for a lane: start / real bits and the V value / column
-// pairs (baked layouts: value and x halves).  Loaded a window ahead of their use so that
-// the stream latency overlaps the previous window's x gathers.
+// pairs (baked layouts: value and x halves), requested together.
 template <class VT, class IT, int VM, bool BAKED>
 struct WinData {
     uint32_t sraw, rraw;
@@ -544,7 +543,7 @@ __device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int la
 // positions per lane for direct layouts and the upper bound of th for tiled ones.  PADDED:
 // the layout has padding positions (real-bit map).  EMPTY: some rows are empty.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
-          bool BAKED, bool PADDED, bool EMPTY, bool PF = false>
+          bool BAKED, bool PADDED, bool EMPTY>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 {
     const int lane = threadIdx.x & 31;
@@ -566,20 +565,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
         uint32_t cnt = __ldg(a.wcount + w0);  // row starts before this range
         bool seen = (w0 == 0);                // a row start has been met in the range
         AT carry = (AT)0;
-        // PF: the next window's bits and streams are requested before this window's x
-        // gathers, so that their latency overlaps the gathers and the row sums
-        WinData<VT, IT, VM, BAKED> nxt;
-        if constexpr (PF) load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w0, lane, V, nxt);
         for (uint32_t w = w0; w < w1; w++) {
             // bits and streams are requested together (the streams do not wait for the
             // bits), then the x gathers
             WinData<VT, IT, VM, BAKED> cur;
-            if constexpr (PF) {
-                cur = nxt;
-                if (w + 1 < w1) load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w + 1, lane, V, nxt);
-            } else {
-                load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w, lane, V, cur);
-            }
+            load_win<VT, IT, VM, TILED, BAKED, PADDED>(a, w, lane, V, cur);
             const uint32_t W = w * WS;
             const WinCtl ctl = window_ctl(lane, W, V, FULLV, a.npos, cur.sraw, seen, false);
             if (ctl.skip) continue;  // all of it continues an earlier warp's row
@@ -1079,14 +1069,13 @@ gs_status launch_k(const RowsArgs &a, bool padded, cudaStream_t s)
     uint32_t blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
     blocks = min(blocks, 148u * 256u);
     const bool empty = a.n_empty != 0;
-    // tiled layouts of tileH 2..4 load their streams a window ahead (COM on the power-law:
-    // th=2 575 -> 528 us, th=4 423 -> 399 us; on the 27-point stencil: th=2 860 -> 775 us,
-    // th=4 564 -> 500 us).  With tileH 5..8 (94 registers against 64) and on the direct
-    // layouts (80 against 48) the lost blocks per SM cost more than the overlap gains.
-    constexpr bool kPrefetch = TILED && VM <= 4;
+    // Loading a window's streams a window ahead paid for tileH 2..4 while the tiled slots
+    // were found by dividing by the tile size (COM th=4 on the power-law 423 -> 399 us); with
+    // the division gone the 64 registers it needs cost more than it hides (power-law COM
+    // th=4 380 -> 364 us without it, th=2 500 -> 476; drop-in gaxtch th=4 326 -> 295;
+    // 27-point stencil th=4 478 -> 454), so every window loads just before its use.
 #define GS_L(P, E)                                                                          \
-    k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E, kPrefetch>                        \
-        <<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
+    k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
     if (padded) {
         if (empty) GS_L(true, true); else GS_L(true, false);
     } else {
