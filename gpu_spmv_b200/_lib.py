@@ -158,7 +158,7 @@ class MatrixInfo(C.Structure):
                 ("d_brp", C.c_void_p), ("d_mapx", C.c_void_p), ("d_permi", C.c_void_p),
                 ("d_nmc", C.c_void_p), ("d_chp", C.c_void_p), ("d_rpos", C.c_void_p),
                 ("d_rlen", C.c_void_p), ("conv_ms", C.c_double), ("mfp", C.c_double),
-                ("beta", C.c_double), ("lane_positions", UIN)]
+                ("beta", C.c_double), ("lane_positions", UIN), ("tiles_per_step", UIN)]
 
 
 _vp = C.c_void_p

@@ -140,6 +140,9 @@ gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *i)
     i->mfp = A->mfp;
     i->beta = A->beta;
     i->lane_positions = (A->p.format == GS_FMT_K1 || A->tile_w) ? 0u : A->plan.V;
+    i->tiles_per_step = 0;
+    if (A->tiled && A->plan.aligned && A->p.tileHW == 32 && (A->p.tileH == 2 || A->p.tileH == 4))
+        i->tiles_per_step = A->plan.grouped ? 2u : 1u;
     return GS_OK;
 }
 

@@ -545,8 +545,10 @@ gs_status convert(gs_matrix *A, const gs_convert_params &p, uint32_t n, uint32_t
             }
         }
         GS_TRY(build_rows_plan(A->rpos.as<uint32_t>(), need_rlen ? A->rlen.as<uint32_t>() : nullptr,
-                               n, V, A->plan, s));
+                               n, V, A->plan, s, A->tiled));
         A->plan.aligned = aligned;
+        if (A->tiled && aligned && (th == 2 || th == 4))
+            GS_TRY(random_columns(d_row, d_col, n, &A->plan.grouped, s));
         // FP64 whole-tile layouts: the same rows over tiles for the tile kernel (windows of
         // one 32-tile chunk).  Widths 4-16 only: at 32 a tile spans 16 lanes and 16 load
         // steps, too few gathers in flight per lane (power-law AXC hbs 32: 846 us on the

@@ -123,7 +123,7 @@ namespace gs {
 //  aligned: every row starts on a multiple of V positions (UNC / AXC layouts)
 struct RowsPlan {
     uint32_t npos = 0, nwin = 0, V = 8, wpw = 4, n_empty = 0;
-    bool padded = false, aligned = false;
+    bool padded = false, aligned = false, grouped = false;
     DevBuf sbits, rbits, wcount, ne, empty, colbase, status;
 };
 }  // namespace gs
@@ -200,6 +200,7 @@ struct RowsArgs {
     uint32_t n_empty;
     uint32_t aligned;              // rows start on multiples of V (aligned kernel applies)
     uint32_t wide;                 // val and col 32-byte aligned: 32-byte stream loads
+    uint32_t grouped;              // x gathers close to random: owned tiles go two at a time
     const uint32_t *sbits, *rbits, *wcount, *ne, *empty, *colbase;
     uint32_t *status;  // device status word (bounded-wait timeouts)
     const void *val;   // value stream (or the baked ax)
@@ -217,13 +218,17 @@ constexpr uint32_t kDirectV = 8;
 // with local columns: more bytes in flight per warp).
 gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
                                 uint64_t nnz, uint32_t *V, cudaStream_t s);
+// Whether the x gathers of a CSR matrix are close to random: fewer than a quarter of a
+// sample of in-row column steps (up to 32 steps of 65,536 rows) stay within 16 columns.
+gs_status random_columns(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
+                         bool *random, cudaStream_t s);
 // Positions per lane for a layout whose rows start on multiples of `align` positions
 // (0: no alignment): returns the V that makes the aligned kernel apply, or kDirectV.
 uint32_t aligned_lane_positions(uint32_t align, bool *aligned);
 // Build the plan from a row table: rpos[0..n] first position of each row (rpos[n] = total
 // positions), rlen[r] real length (nullptr when rows carry no padding).
 gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
-                          uint32_t V, RowsPlan &P, cudaStream_t s);
+                          uint32_t V, RowsPlan &P, cudaStream_t s, bool tiled = false);
 // 16-bit column offsets: per-window base over real positions, col16 = col32 - base.
 gs_status build_u16_columns(const uint32_t *d_col32, uint32_t nslots, RowsPlan &P,
                             uint16_t *d_col16, cudaStream_t s);

@@ -630,7 +630,7 @@ static str_res run_baked(const char *name, UIN nrows, UIN nnz, const FPT *hax, U
     if (tiled) aligned = align != 0 && (th == 2 || th == 4 || th == 8 || th == 16);
     else if (align) V = gs::aligned_lane_positions(align, &aligned);
     if (h2d(ax, hax, lenAX) || y.alloc((size_t)nrows * 8) ||
-        gs::build_rows_plan(rpos.as<UIN>(), nullptr, nrows, V, P, 0))
+        gs::build_rows_plan(rpos.as<UIN>(), nullptr, nrows, V, P, 0, tiled))
         return error_res(name, gs_last_error());
     P.aligned = aligned;
     gs::RowsArgs a = gs::rows_args(P);

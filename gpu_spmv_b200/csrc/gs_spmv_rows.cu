@@ -587,6 +587,93 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 }
 
 // ---------------------------------------------------------------------------------------
+// NT consecutive 32-wide tiles w .. w+NT-1 (window = tile, lane l owns tile column l, V =
+// tileH positions of one row) that a warp owns outright: a row start was met before them
+// and all lie inside its range.  The column loads and x gathers of all NT tiles issue
+// before any sum and their segmented scans interleave, so a lane keeps NT*V gathers in
+// flight where one tile gives V.  The value loads issue after the gathers: they arrive
+// while the gathers are in flight, and their registers are not held across the column
+// round trip.  Each tile's sums, and their order, are those of the single-tile path.
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, int NT,
+          bool PADDED, bool EMPTY>
+__device__ __forceinline__ void owned_tiles(const RowsArgs &a, YT *y, int lane, unsigned mine,
+                                            uint32_t w, uint32_t &cnt, AT &carry)
+{
+    constexpr uint32_t WS = 32u * V;
+    constexpr uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
+    const VT *val = static_cast<const VT *>(a.val);
+    const IT *col = static_cast<const IT *>(a.col);
+    const XT *x = static_cast<const XT *>(a.x);
+    IT c[NT][V];
+    uint32_t rb[NT];
+    unsigned smask[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        const uint32_t s0 = (w + (uint32_t)t) * WS + (uint32_t)lane;
+#pragma unroll
+        for (int k = 0; k < V; k++) c[t][k] = ld_stream(col + s0 + 32u * (uint32_t)k);
+        // V divides 32 and qb is a multiple of V: the lane's bits sit in one word
+        const uint32_t qb = (w + (uint32_t)t) * WS + (uint32_t)lane * V;
+        const bool inb = qb < a.npos;
+        rb[t] = inb ? FULLV : 0u;
+        if constexpr (PADDED)
+            rb[t] = inb ? ((__ldg(a.rbits + (qb >> 5)) >> (qb & 31)) & FULLV) : 0u;
+        smask[t] = __ballot_sync(kFull, inb && ((__ldg(a.sbits + (qb >> 5)) >> (qb & 31)) & 1u));
+    }
+    XT xv[NT][V];
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+        for (int k = 0; k < V; k++)
+            xv[t][k] = ((rb[t] >> k) & 1u) ? __ldg(x + (uint32_t)c[t][k]) : (XT)0;
+    VT v[NT][V];
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+        for (int k = 0; k < V; k++)
+            v[t][k] = ld_stream(val + (w + (uint32_t)t) * WS + (uint32_t)lane + 32u * (uint32_t)k);
+    AT S[NT];
+    int sstart[NT];
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        AT acc = (AT)0;
+#pragma unroll
+        for (int k = 0; k < V; k++)
+            acc = add_rn(acc, (AT)(((rb[t] >> k) & 1u)
+                                       ? mul_rn((PT)ValTraits<VT>::to_f64(v[t][k]), (PT)xv[t][k])
+                                       : (PT)0));
+        S[t] = acc;
+        const unsigned le = smask[t] & mine;
+        sstart[t] = le ? 31 - __clz(le) : -1;
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            AT u = __shfl_up_sync(kFull, S[t], d);
+            if (lane >= d && lane - d >= sstart[t]) S[t] = add_rn(S[t], u);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+        if (sstart[t] < 0) S[t] = add_rn(S[t], carry);
+        const uint32_t qb = (w + (uint32_t)t) * WS + (uint32_t)lane * V;
+        bool nxt;
+        if (lane < 31) nxt = (smask[t] >> (lane + 1)) & 1u;
+        else if (t + 1 < NT) nxt = smask[t + 1] & 1u;  // lane 0 of the next tile
+        else nxt = (qb + V < a.npos) ? ((__ldg(a.sbits + ((qb + V) >> 5)) >> ((qb + V) & 31)) & 1u)
+                                     : true;
+        if (qb + V >= a.npos) nxt = true;
+        if (qb < a.npos && nxt) {
+            const uint32_t rank = cnt + (uint32_t)__popc(smask[t] & mine) - 1u;
+            store_y<YT, AT>(y + (EMPTY ? __ldg(a.ne + rank) : rank), S[t]);
+        }
+        carry = __shfl_sync(kFull, S[t], 31);
+        cnt += (uint32_t)__popc(smask[t]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Aligned kernel.  In the UNC layouts every row starts on a tile column (tileH > 1: a
 // multiple of th positions) or a tile (tileH = 1: a multiple of tileHW), and in AXC on a
 // brick: with V positions per lane and V dividing that alignment, a lane never holds two
@@ -598,9 +685,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 // T32: tiled layouts with tileHW = 32 and tileH = V, where a window of 32 lanes x V positions
 // is exactly one tile and lane l owns its column l: element k of that column is slot
 // w * 32V + 32k + l, with no division by the runtime tile size.
+//
+// NT > 1 (32-wide run-time-x tiles of tileH 2 and 4, x gathers close to random): the
+// windows a warp owns outright go NT at a time through owned_tiles.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
-          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false, bool EARLY = false>
-__global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
+          bool BAKED, bool PADDED, bool EMPTY, bool T32, bool EARLY, int NT>
+__device__ __forceinline__ void rows_aligned(const RowsArgs &a)
 {
     const int lane = threadIdx.x & 31;
     YT *y = static_cast<YT *>(a.y);
@@ -626,6 +716,15 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
         bool seen = (w0 == 0);
         AT carry = (AT)0;
         for (uint32_t w = w0; w < a.nwin; w++) {
+            if constexpr (NT > 1) {
+                static_assert(EARLY && !BAKED, "tile groups are for 32-wide run-time-x tiles");
+                if (seen && w + NT <= w1) {
+                    owned_tiles<VT, IT, XT, PT, AT, YT, V, NT, PADDED, EMPTY>(a, y, lane, mine, w,
+                                                                           cnt, carry);
+                    w += NT - 1;
+                    continue;
+                }
+            }
             const bool over = w >= w1;
             if (over && !seen) break;
             const uint32_t qb = w * WS + (uint32_t)lane * V;
@@ -770,6 +869,25 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
             if (over && smask != 0u) break;  // the range's last row ended in this window
         }
     }
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false, bool EARLY = false>
+__global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
+{
+    rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, PADDED, EMPTY, T32, EARLY, 1>(a);
+}
+
+// Two owned tiles per step.  Register caps: 48 for tileH = 4 (5 blocks of 256 per SM), 40
+// for tileH = 2 (6 blocks); uncapped the compiler takes 56-64 and the x gathers in flight
+// per SM fall.
+constexpr int kGroupTiles = 2;
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool PADDED,
+          bool EMPTY>
+__global__ void __launch_bounds__(256, V == 2 ? 6 : 5) k_rows_grouped(const RowsArgs a)
+{
+    rows_aligned<VT, IT, XT, PT, AT, YT, V, true, false, PADDED, EMPTY, true, true,
+                 kGroupTiles>(a);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1102,6 +1220,23 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
     // th=4 334 -> 289, th=8 412 -> 322; the same bits).  The direct layouts keep the
     // dependent loads: there the early loads cost 8 registers (48 for 8 positions per
     // lane) and AXC on the power-law went 461 -> 558 us.
+    // random x gathers on 32-wide tiles of tileH 2 or 4: two owned tiles per step
+    // (power-law UNC th=4 318 -> 303 us, th=2 352 -> 326, the same bits; on the 27-point
+    // stencil, whose gathers mostly hit lines already in L1, one tile per step stays faster:
+    // th=4 276 against 301 us)
+    if constexpr (TILED && !BAKED && (V == 2 || V == 4)) {
+        if (t32 && a.grouped) {
+#define GS_G(P, E) k_rows_grouped<VT, IT, XT, PT, AT, YT, V, P, E><<<blocks, 256, 0, s>>>(a)
+            if (padded) {
+                if (empty) GS_G(true, true); else GS_G(true, false);
+            } else {
+                if (empty) GS_G(false, true); else GS_G(false, false);
+            }
+#undef GS_G
+            GS_CHECK_LAUNCH();
+            return GS_OK;
+        }
+    }
 #define GS_L(P, E)                                                                          \
     do {                                                                                    \
         if (t32)                                                                            \
@@ -1452,15 +1587,11 @@ gs_status launch_tiles_t(const RowsArgs &a, cudaStream_t s)
 
 }  // namespace
 
-gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
-                                uint64_t nnz, uint32_t *V, cudaStream_t s)
+gs_status random_columns(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
+                         bool *random, cudaStream_t s)
 {
-    *V = kDirectV;
-    if (n == 0 || nnz == 0) return GS_OK;
-    if ((double)nnz / (double)n < 8.0) {  // short rows: more warps beat longer lanes
-        *V = 4;
-        return GS_OK;
-    }
+    *random = false;
+    if (n == 0) return GS_OK;
     const uint32_t samples = n < 65536u ? n : 65536u;
     const uint32_t stride = n / samples;
     DevBuf cnt;
@@ -1471,14 +1602,28 @@ gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, ui
     unsigned long long h[2] = {0, 0};
     GS_CUDA(cudaMemcpyAsync(h, cnt.p, 16, cudaMemcpyDeviceToHost, s));
     GS_CUDA(cudaStreamSynchronize(s));
-    // fewer than a quarter of the steps stay within a line: the x gathers are (close to)
-    // random and set the pace
-    if (h[1] * 4 < h[0]) *V = 4;
+    *random = h[1] * 4 < h[0];
+    return GS_OK;
+}
+
+gs_status direct_lane_positions(const uint32_t *d_row, const uint32_t *d_col, uint32_t n,
+                                uint64_t nnz, uint32_t *V, cudaStream_t s)
+{
+    *V = kDirectV;
+    if (n == 0 || nnz == 0) return GS_OK;
+    if ((double)nnz / (double)n < 8.0) {  // short rows: more warps beat longer lanes
+        *V = 4;
+        return GS_OK;
+    }
+    // random x gathers set the pace: 4 positions per lane
+    bool rnd = false;
+    GS_TRY(random_columns(d_row, d_col, n, &rnd, s));
+    if (rnd) *V = 4;
     return GS_OK;
 }
 
 gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32_t n,
-                          uint32_t V, RowsPlan &P, cudaStream_t s)
+                          uint32_t V, RowsPlan &P, cudaStream_t s, bool tiled)
 {
     P.V = V;
     P.padded = d_rlen != nullptr;
@@ -1490,9 +1635,13 @@ gs_status build_rows_plan(const uint32_t *d_rpos, const uint32_t *d_rlen, uint32
     P.nwin = (uint32_t)(((uint64_t)npos + WS - 1) / WS);
     // windows per warp range of the LDG kernels: ~2048 positions at 8 per lane (27-point
     // stencil against ~1024: CSR 330 -> 318 us, COM th=8 547 -> 471, UNC th=8 448 -> 408;
-    // power-law: COM th=8 437 -> 409, UNC th=8 364 -> 343), ~1024 otherwise; fewer when the
-    // matrix is too small to give every SM enough warps
-    uint32_t wpw = (uint32_t)(((V == 8 ? 2048u : 1024u) + WS - 1) / WS);
+    // power-law: COM th=8 437 -> 409, UNC th=8 364 -> 343) and for tiled layouts of tileH
+    // 2-4 (27-point stencil: COM th=4 452 -> 420 us, UNC th=4 288 -> 276; drop-in gaxtch
+    // th=4 on the power-law 295 -> 281), ~1024 otherwise (CSR at 4 per lane on the
+    // power-law: 329 against 334 us); fewer when the matrix is too small to give every SM
+    // enough warps
+    const uint32_t range = (V == 8 || (tiled && V <= 4)) ? 2048u : 1024u;
+    uint32_t wpw = (uint32_t)((range + WS - 1) / WS);
     while (wpw > 1 && (uint64_t)P.nwin / wpw < 148ull * 48ull) wpw >>= 1;
     P.wpw = wpw;
     const size_t words = (size_t)P.nwin * V + 2;
@@ -1575,6 +1724,7 @@ RowsArgs rows_args(const RowsPlan &P)
 {
     RowsArgs a{};
     a.aligned = P.aligned ? 1u : 0u;
+    a.grouped = P.grouped ? 1u : 0u;
     a.npos = P.npos;
     a.nwin = P.nwin;
     a.wpw = P.wpw;

@@ -304,6 +304,9 @@ typedef struct {
     double beta;    /* occupancy nnz / stored slots */
     UIN lane_positions; /* consecutive positions per lane of the row-stream kernel (0: the
                          * matrix runs on the K1 or the tile kernel) */
+    UIN tiles_per_step; /* UNC layouts of 32-wide tiles, tileH 2 or 4: tiles a warp takes
+                         * per step (2 when the x gathers are close to random, else 1);
+                         * 0 for every other layout */
 } gs_matrix_info;
 gs_status gs_matrix_get_info(const gs_matrix *A, gs_matrix_info *info);
 

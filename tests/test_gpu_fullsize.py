@@ -158,3 +158,36 @@ def test_stencil27_160_row_stream(port):
             assert A.info.lane_positions == 8
         _check(port, row, col, val, x, A.spmv(torch.from_numpy(x).cuda()).cpu().numpy())
         A.close()
+
+
+@pytest.mark.parametrize("th", [2, 4])
+def test_grouped_tiles_random_rows(port, th):
+    """UNC layouts of 32-wide tiles, tileH 2 and 4, on a matrix with random columns (the
+    row-stream kernel then takes the tiles a warp owns two at a time): 1.5M rows of 0-40
+    elements (empty rows included) and 16 rows of 20k-200k elements that cross many tiles
+    and warp ranges, within 1e-13 (|A||x|)_i of the oracle; the 27-point stencil's local
+    columns keep one tile per step."""
+    from gpu_spmv_b200 import engine as E
+    from gpu_spmv_b200 import matgen
+
+    rng = np.random.default_rng(11)
+    n = 1_500_000
+    lens = rng.integers(0, 41, n)
+    lens[rng.choice(n, 16, replace=False)] = rng.integers(20_000, 200_000, 16)
+    row = np.zeros(n + 1, dtype=np.uint32)
+    row[1:] = np.cumsum(lens)
+    nnz = int(row[-1])
+    col = rng.integers(0, n, nnz, dtype=np.uint32)
+    val = rng.uniform(-1.0, 1.0, nnz)
+    x = rng.uniform(-1.0, 1.0, n)
+    A = E.Matrix(row, col, val, ncols=n, fmt="AXT", mode="UNC", tileH=th, tileHW=32)
+    assert A.info.tiles_per_step == 2
+    _check(port, row, col, val, x, A.spmv(torch.from_numpy(x).cuda()).cpu().numpy())
+    A.close()
+    srow, scol, sval = matgen.stencil27(40, seed=2)
+    S = E.Matrix(srow, scol, sval, ncols=len(srow) - 1, fmt="AXT", mode="UNC", tileH=th,
+                 tileHW=32)
+    assert S.info.tiles_per_step == 1
+    sx = matgen.vector(len(srow) - 1, "normal", seed=2)
+    _check(port, srow, scol, sval, sx, S.spmv(torch.from_numpy(sx).cuda()).cpu().numpy())
+    S.close()
