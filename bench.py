@@ -116,8 +116,8 @@ def variant_bytes(n: int, nnz: int, kw: dict, run: dict) -> float:
     return E.algorithmic_bytes(n, n, nnz, 1, s_v, s_i, s_x, s_y)
 DEFAULT_VARIANT = "k1"
 # formats timed beside the headline (µs per product), same matrix and x
-COMPARE = ("csr", "axt-com-th1", "axt-unc-th1-hw4", "axt-unc-th4", "axt-unc-th8", "axc",
-           "axcv0", "axcv1", "axbv0")
+COMPARE = ("csr", "axt-com-th1", "axt-com-th4", "axt-unc-th1-hw4", "axt-unc-th2", "axt-unc-th4",
+           "axt-unc-th8", "axc", "axcv0", "axcv1", "axbv0")
 
 
 def make_matrix(workload: str, rank: int, matgen=None):
@@ -645,14 +645,15 @@ def time_gathers(workload: str):
     return out
 
 
-def gather_ceiling(A, n, nnz, kw, dx, kern_ms):
+def gather_ceiling(A, n, nnz, kw, dx, kern_ms, rate_per_s=None):
     """The product's line requests per launch against this GPU's measured rate of random
-    8-byte reads from x (gsp_gather_rate on the workload's own x): one request per x gather
-    (nnz), the value and column streams (slots x bytes / 128), and y (one request per row when
-    K1 scatters it by its permutation, else streamed).  frac = ceiling time / kernel time."""
+    8-byte reads from x (gsp_gather_rate on the workload's own x, or `rate_per_s` when it was
+    measured already): one request per x gather (nnz), the value and column streams (slots x
+    bytes / 128), and y (one request per row when K1 scatters it by its permutation, else
+    streamed).  frac = ceiling time / kernel time."""
     import ctypes as Cc
 
-    rate = Cc.c_double(gather_rate(dx, n))
+    rate = Cc.c_double(rate_per_s if rate_per_s else gather_rate(dx, n))
     slots = nnz / A.info.beta if A.info.beta > 0 else nnz
     sv = {"f64": 8, "f32": 4, "bf16": 2}[kw.get("vtype", "f64")]
     si = 2 if kw.get("itype") == "u16" else 4
@@ -712,7 +713,8 @@ def time_formats(row, col, val, x, steps: int):
     n = len(row) - 1
     dx = torch.from_numpy(x).cuda()
     dy = torch.empty(n, dtype=torch.float64, device="cuda")
-    out, errs = {}, {}
+    out, errs, fracs = {}, {}, {}
+    rate = gather_rate(dx, n)
     for vname in COMPARE:
         kw = dict(VARIANTS[vname])
         A = E.Matrix(row, col, val, ncols=n, **kw)
@@ -727,6 +729,9 @@ def time_formats(row, col, val, x, steps: int):
             ts.append((a, b))
         torch.cuda.synchronize()
         out[vname] = round(1e3 * sum(a.elapsed_time(b) for a, b in ts) / steps, 2)
+        if kw.get("vtype", "f64") == "f64":
+            fracs[vname] = round(gather_ceiling(A, n, len(col), kw, dx, out[vname] * 1e-3,
+                                                rate)["frac"], 3)
         A.close()
         errs[vname] = error_vs_fp64(row, col, val, x, dy)
     # cuSPARSE generic CSR SpMV through the drop-in test_gcucsr (per-launch events)
@@ -741,6 +746,7 @@ def time_formats(row, col, val, x, steps: int):
     finally:
         L.lib().gs_set_num_ite(old)
     out["error_vs_fp64"] = errs
+    out["gather_ceiling_frac"] = fracs
     return out
 
 
