@@ -15,7 +15,10 @@ is inserted between steps.
 
 Under torchrun (N > 1) every rank owns an independent partition of the same size (its own
 power-law block, seed 1 + rank: a block-diagonal operator, no exchange on the data path),
-so per-GPU work is fixed ("weak" scaling); the time is the max over ranks.
+so per-GPU work is fixed ("weak" scaling); the time is the max over ranks.  Beside it the
+line's "dist" object times the partitioned product of ONE shared matrix (DistSpMV:
+nnz-balanced row blocks, x all-gathered over NCCL, each block in K1), µs per product as the
+max over ranks ("strong" scaling).
 ``--impl reference`` times the reference's own CPU CSR SpMV (ncsr, cudaSpmv.cu:451,
 compiled unchanged into oracle/_ref) on the host cores, rank 0 only.
 """
@@ -750,6 +753,65 @@ def time_formats(row, col, val, x, steps: int):
     return out
 
 
+def time_dist(row, col, val, x, steps: int, warmup: int, device, local_factory=None,
+              group=None):
+    """The distributed product of ONE matrix shared by every rank
+    (gpu_spmv_b200.distributed.DistSpMV: nnz-balanced row blocks, x all-gathered over the
+    process group, each rank's block multiplied on its own device): µs per product, the max
+    over ranks, timed with CUDA events on CUDA devices (the wall clock on CPU ranks).  Before
+    any timed collective every rank reports whether it built its block (one all-reduce), so
+    that no rank enters the timed all-gathers alone; on a failure every rank returns
+    {"error": ...}.  `row` None stands for a matrix this rank could not build."""
+    import torch
+    import torch.distributed as dist
+
+    from gpu_spmv_b200.distributed import DistSpMV
+
+    err, D, xl = None, None, None
+    try:
+        if row is None:
+            raise RuntimeError("no matrix")
+        D = DistSpMV(row, col, val, len(row) - 1, group=group, device=device,
+                     local_factory=local_factory)
+        xl = torch.from_numpy(np.ascontiguousarray(x[D.r0:D.r1])).to(device)
+    except Exception as e:
+        err = f"{type(e).__name__}: {e}"
+    flag = torch.tensor([0 if err else 1], dtype=torch.int32, device=device)
+    dist.all_reduce(flag, op=dist.ReduceOp.MIN, group=group)
+    if int(flag.item()) == 0:
+        return {"error": err or "another rank could not build its row block"}
+    cuda = torch.device(device).type == "cuda"
+    for _ in range(warmup):
+        D.spmv(xl)
+    if cuda:
+        torch.cuda.synchronize()
+    dist.barrier(group=group)
+    if cuda:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            D.spmv(xl)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+    else:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            D.spmv(xl)
+        ms = (time.perf_counter() - t0) * 1e3
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    us = float(t.item()) * 1e3 / steps
+    nnz = len(col)
+    row64 = np.asarray(row, dtype=np.int64)
+    return {"us_per_product": round(us, 2), "gflops": round(2.0 * nnz / (us * 1e-6) / 1e9, 1),
+            "ranks": D.world, "rows_per_rank": D.sizes,
+            "nnz_per_rank": [int(row64[D.bounds[k + 1]] - row64[D.bounds[k]])
+                             for k in range(D.world)],
+            "allgather_bytes_per_product": D.pad * D.world * xl.element_size(),
+            "local_format": "K1", "scaling": "strong", "steps": steps, "warmup": warmup}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -992,6 +1054,21 @@ def run_ours(args):
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
+    # the partitioned product of one shared matrix (x all-gather over NCCL), beside the
+    # independent per-rank blocks of the headline
+    dres = None
+    if dist and not args.no_dist:
+        try:
+            drow, dcol, dval, dxv = make_matrix(args.workload, 0)
+        except Exception:
+            drow = dcol = dval = dxv = None
+        dres = time_dist(drow, dcol, dval, dxv, K, args.warmup, torch.device("cuda", local))
+        if drow is not None:
+            dres["workload"] = (f"{WORKLOADS[args.workload]['desc']}, seed "
+                                f"{WORKLOADS[args.workload]['seed']}, one matrix shared by "
+                                f"the {world} ranks")
+        del drow, dcol, dval, dxv
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1018,6 +1095,7 @@ def run_ours(args):
         "mixed": mixed,
         "adjoint": adjoint,
         "batched": batched,
+        "dist": dres,
         "gpu_launches": K,
         "clocks": clocks,
     }
@@ -1035,6 +1113,8 @@ def main():
     ap.add_argument("--variant", default=DEFAULT_VARIANT, choices=list(VARIANTS))
     ap.add_argument("--sweep", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-dist", action="store_true",
+                    help="under torchrun: skip the partitioned product of one shared matrix")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-formats", action="store_true")

@@ -100,6 +100,78 @@ def test_gloo_two_ranks(name):
     mp.spawn(_rank_main, args=(2, _free_port(), name, 11), nprocs=2, join=True)
 
 
+class FailingLocal:
+    """A local operator that cannot be built (a rank whose block fails)."""
+
+    def __init__(self, *args):
+        raise RuntimeError("this rank's block could not be built")
+
+
+def _bench_rank_main(rank, world, port, fail_rank):
+    import sys
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        rng = np.random.default_rng(5)
+        row, col, val = case("powerlaw_small", rng)
+        n = len(row) - 1
+        x = rng.uniform(-1, 1, n)
+        factory = FailingLocal if rank == fail_rank else OracleLocal
+        out = bench.time_dist(row, col, val, x, 3, 1, "cpu", local_factory=factory)
+        if fail_rank >= 0:
+            assert set(out) == {"error"}, out
+            if rank == fail_rank:
+                assert "could not be built" in out["error"]
+        else:
+            assert "error" not in out, out
+            assert out["ranks"] == world and sum(out["rows_per_rank"]) == n
+            assert sum(out["nnz_per_rank"]) == len(col)
+            assert out["us_per_product"] > 0 and out["scaling"] == "strong"
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fail_rank", [-1, 1], ids=["both_build", "rank1_fails"])
+def test_bench_dist_two_ranks(fail_rank):
+    """bench.time_dist over two gloo ranks: the shared matrix's row blocks cover it, the time
+    is reported; a rank that cannot build its block makes every rank return the error
+    instead of entering the timed all-gathers alone."""
+    import torch.multiprocessing as mp
+
+    mp.spawn(_bench_rank_main, args=(2, _free_port(), fail_rank), nprocs=2, join=True)
+
+
+@pytest.mark.gpu
+def test_bench_dist_one_nccl_rank():
+    """bench.time_dist on one NCCL rank with the engine's K1 block on the GPU."""
+    import sys
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0,
+                            world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        rng = np.random.default_rng(3)
+        row, col, val = case("powerlaw_small", rng)
+        n = len(row) - 1
+        out = bench.time_dist(row, col, val, rng.uniform(-1, 1, n), 5, 2,
+                              torch.device("cuda", 0))
+        assert "error" not in out, out
+        assert out["rows_per_rank"] == [n] and out["gflops"] > 0
+    finally:
+        dist.destroy_process_group()
+
+
 @pytest.mark.gpu
 def test_nccl_one_rank_engine(port):
     import torch.distributed as dist
