@@ -162,6 +162,7 @@ def apply_config(batch: E.Batch, config: dict) -> bool:
 FORMAT_CANDIDATES = {
     "k1": dict(fmt="K1"),
     "csr": dict(fmt="CSR"),
+    "axt-unc-th2": dict(fmt="AXT", mode="UNC", tileH=2, tileHW=32),
     "axt-unc-th4": dict(fmt="AXT", mode="UNC", tileH=4, tileHW=32),
     "axt-unc-th8": dict(fmt="AXT", mode="UNC", tileH=8, tileHW=32),
     "axt-unc-th1-hw4": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
