@@ -238,8 +238,16 @@ __device__ __forceinline__ WinCtl window_ctl(int lane, uint32_t W, uint32_t V, u
     return c;
 }
 
+// Row ranks by ballots, one per bit of the lanes' counts of row starts (BR), or by a shuffle
+// scan of those counts: the same ranks.  Ballots ran faster for tiled layouts of 8 positions
+// per lane (COM th=8: power-law 394 -> 345 us, 27-point stencil 450 -> 393) and for direct
+// layouts of 4 (CSR on the power-law 329 -> 324), slower for direct layouts of 8 (CSR on the
+// stencil 321 -> 333) and tiled ones of 4 (COM th=4 on the power-law 358 -> 380) and 16 (COM
+// th=16 624 -> 872).
+template <int VM, bool TILED> constexpr bool kBallotRanks = TILED ? VM == 8 : VM == 4;
+
 // Row ranks, sequential lane sums, segmented warp scan, y writes and the window carry.
-template <class AT, class YT, int VM, bool EMPTY, class PT>
+template <class AT, class YT, int VM, bool EMPTY, class PT, bool BR>
 __device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane, uint32_t W,
                                               uint32_t V, uint32_t sraw, uint32_t vmask,
                                               uint32_t rb, const PT (&prod)[VM], uint32_t &cnt,
@@ -248,15 +256,32 @@ __device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane
     const uint32_t qb = W + (uint32_t)lane * V;
     const uint32_t sb = sraw & vmask;
     const int c0 = __popc(sb);
-    int inc = c0;
+    // inc: row starts of the window up to and including the lane's; nxt_lane: bit 0 is
+    // whether the next lane's first position starts a row
+    int inc;
+    uint32_t total, nxt_lane;
+    if constexpr (BR) {
+        constexpr int kCountBits = VM >= 16 ? 5 : (VM >= 8 ? 4 : (VM >= 4 ? 3 : (VM >= 2 ? 2 : 1)));
+        const unsigned below = (1u << lane) - 1u;
+        inc = c0;
+        total = 0;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        int t = __shfl_up_sync(kFull, inc, d);
-        if (lane >= d) inc += t;
+        for (int bit = 0; bit < kCountBits; bit++) {
+            const unsigned B = __ballot_sync(kFull, (c0 >> bit) & 1);
+            inc += __popc(B & below) << bit;
+            total += (uint32_t)__popc(B) << bit;
+        }
+        nxt_lane = __ballot_sync(kFull, sraw & 1u) >> ((lane + 1) & 31);
+    } else {
+        inc = c0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int t = __shfl_up_sync(kFull, inc, d);
+            if (lane >= d) inc += t;
+        }
+        total = (uint32_t)__shfl_sync(kFull, inc, 31);
+        nxt_lane = __shfl_down_sync(kFull, sraw, 1);
     }
-    const uint32_t total = (uint32_t)__shfl_sync(kFull, inc, 31);
-    // whether the row in progress at the lane's last position ends there
-    const uint32_t nxt_lane = __shfl_down_sync(kFull, sraw, 1);
     const uint32_t nxt_win = (lane == 31) ? get_bits(a.sbits, W + 32u * V, 1) : 0u;
 
     const bool has = vmask != 0u;
@@ -531,8 +556,8 @@ __device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int la
         const uint32_t rb = PADDED ? (get_bits(a.rbits, qb, V) & ctl.vmask) : ctl.vmask;
         PT prod[VM];
         products_ldg<VT, IT, XT, PT, VM, TILED, BAKED>(a, w, qb, V, rb, prod);
-        window_reduce<AT, YT, VM, EMPTY, PT>(a, y, lane, W, V, sraw, ctl.vmask, rb, prod, cnt,
-                                             carry);
+        window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>>(
+            a, y, lane, W, V, sraw, ctl.vmask, rb, prod, cnt, carry);
         if (ctl.slanes != 0u) break;  // the last row ended in this window
     }
 }
@@ -576,8 +601,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
             const uint32_t rb = cur.rraw & ctl.vmask;
             PT prod[VM];
             win_products<VT, IT, XT, PT, VM, BAKED>(a, w, V, cur, rb, prod);
-            window_reduce<AT, YT, VM, EMPTY, PT>(a, y, lane, W, V, cur.sraw, ctl.vmask, rb,
-                                                 prod, cnt, carry);
+            window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>>(
+                a, y, lane, W, V, cur.sraw, ctl.vmask, rb, prod, cnt, carry);
             seen = true;
         }
         if (seen)
@@ -1160,8 +1185,8 @@ __global__ void __launch_bounds__(kTmaWarps * 32) k_rows_tma(const RowsArgs a)
                                   ? mul_rn((PT)ValTraits<VT>::to_f64(sv[32 * k + lane]), (PT)xv[k])
                                   : (PT)0;
             }
-            window_reduce<AT, YT, TH, EMPTY, PT>(a, y, lane, W, V, sraw, ctl.vmask, rb, prod,
-                                                 cnt, carry);
+            window_reduce<AT, YT, TH, EMPTY, PT, kBallotRanks<TH, true>>(
+                a, y, lane, W, V, sraw, ctl.vmask, rb, prod, cnt, carry);
             seen = true;
         }
         __syncwarp();
