@@ -240,11 +240,12 @@ __device__ __forceinline__ WinCtl window_ctl(int lane, uint32_t W, uint32_t V, u
 
 // Row ranks by ballots, one per bit of the lanes' counts of row starts (BR), or by a shuffle
 // scan of those counts: the same ranks.  Ballots ran faster for tiled layouts of 8 positions
-// per lane (COM th=8: power-law 394 -> 345 us, 27-point stencil 450 -> 393) and for direct
-// layouts of 4 (CSR on the power-law 329 -> 324), slower for direct layouts of 8 (CSR on the
-// stencil 321 -> 333) and tiled ones of 4 (COM th=4 on the power-law 358 -> 380) and 16 (COM
-// th=16 624 -> 872).
-template <int VM, bool TILED> constexpr bool kBallotRanks = TILED ? VM == 8 : VM == 4;
+// per lane (COM th=8: power-law 394 -> 345 us, 27-point stencil 450 -> 393) and of 2 (COM th=2
+// on the power-law 418 -> 404, the stencil 574 -> 577) and for direct layouts of 4 (CSR on the
+// power-law 329 -> 324), slower for direct layouts of 8 (CSR on the stencil 321 -> 333) and
+// tiled ones of 4 (COM th=4 on the power-law 358 -> 380) and 16 (COM th=16 624 -> 872).
+template <int VM, bool TILED>
+constexpr bool kBallotRanks = TILED ? (VM == 8 || VM == 2) : VM == 4;
 
 // Row ranks, sequential lane sums, segmented warp scan, y writes and the window carry.
 template <class AT, class YT, int VM, bool EMPTY, class PT, bool BR>
@@ -1371,6 +1372,10 @@ gs_status launch_shape(const RowsArgs &a, bool tiled, bool padded, uint32_t flag
                 default: break;
                 }
             }
+            // tileH 2 on a kernel of 2 positions per lane, not 4 with half of them idle (40
+            // registers instead of 48: COM th=2 on the power-law 464 -> 416 us, on the 27-point
+            // stencil 702 -> 572; drop-in gaxtch th=2 427 -> 386 and 646 -> 579; same bits)
+            if (a.th <= 2) return launch_k<VT, IT, XT, PT, AT, YT, 2, true, BAKED>(a, padded, s);
             if (a.th <= 4) return launch_k<VT, IT, XT, PT, AT, YT, 4, true, BAKED>(a, padded, s);
             if (a.th <= 8) return launch_k<VT, IT, XT, PT, AT, YT, 8, true, BAKED>(a, padded, s);
             if (a.th <= 16)
