@@ -60,6 +60,7 @@ VARIANTS = {
     "k1": dict(fmt="K1"),
     "axc": dict(fmt="AXC", hbs=32),
     "axt-com-th1": dict(fmt="AXT", mode="COM", tileH=1, tileHW=32, bs=256),
+    "axt-com-th2": dict(fmt="AXT", mode="COM", tileH=2, tileHW=32, bs=256),
     "axt-com-th4": dict(fmt="AXT", mode="COM", tileH=4, tileHW=32, bs=256),
     "axt-com-th8": dict(fmt="AXT", mode="COM", tileH=8, tileHW=32, bs=256),
     "axt-unc-th1-hw4": dict(fmt="AXT", mode="UNC", tileH=1, tileHW=4),
