@@ -255,6 +255,27 @@ def test_lane_positions_choice(port, kind, expect, fmt):
     assert within_bound(y.cpu().numpy(), y_ref, mag)
 
 
+@pytest.mark.parametrize("kind,expect", [("random", 4), ("banded", 8)])
+@pytest.mark.parametrize("fmt", [dict(fmt="AXC", hbs=32),
+                                 dict(fmt="AXT", mode="UNC", tileH=1, tileHW=32)],
+                         ids=["axc32", "unc1hw32"])
+def test_lane_positions_padded32(port, kind, expect, fmt):
+    """Layouts whose rows are padded to 32 positions (AXC hbs 32, UNC tileH 1 tileHW 32)
+    take 4 positions per lane when their x gathers are random, 8 when the columns are local;
+    both within the FP64 bound of the oracle."""
+    from gpu_spmv_b200 import engine as E
+
+    row, col, val = _lane_case(kind)
+    n = len(row) - 1
+    A = E.Matrix(row, col, val, ncols=n, **fmt)
+    assert A._info().lane_positions == expect
+    x = np.random.default_rng(4).uniform(-1, 1, n)
+    y_ref = port.csr_spmv(row, col, val, x)
+    _, mag = port.csr_truth(row, col, val, x)
+    assert within_bound(A.spmv(torch.from_numpy(x).cuda()).cpu().numpy(), y_ref, mag)
+    A.close()
+
+
 @pytest.mark.parametrize("fmt", [dict(fmt="CSR"), dict(fmt="CSR", vtype="f32"),
                                  dict(fmt="AXT", mode="COM", tileH=1, tileHW=32),
                                  dict(fmt="AXT", mode="COM", tileH=4, tileHW=32),
