@@ -1372,9 +1372,10 @@ gs_status launch_shape(const RowsArgs &a, bool tiled, bool padded, uint32_t flag
                 default: break;
                 }
             }
-            // tileH 2 on a kernel of 2 positions per lane, not 4 with half of them idle (40
-            // registers instead of 48: COM th=2 on the power-law 464 -> 416 us, on the 27-point
-            // stencil 702 -> 572; drop-in gaxtch th=2 427 -> 386 and 646 -> 579; same bits)
+            // tileH 2 on a kernel of 2 positions per lane, not 4 with half of them idle (COM
+            // th=2: 46 registers and no spill against 48 and a spill; on the power-law 464 ->
+            // 416 us, on the 27-point stencil 702 -> 572; drop-in gaxtch th=2 427 -> 386 and
+            // 646 -> 579; same bits)
             if (a.th <= 2) return launch_k<VT, IT, XT, PT, AT, YT, 2, true, BAKED>(a, padded, s);
             if (a.th <= 4) return launch_k<VT, IT, XT, PT, AT, YT, 4, true, BAKED>(a, padded, s);
             if (a.th <= 8) return launch_k<VT, IT, XT, PT, AT, YT, 8, true, BAKED>(a, padded, s);
