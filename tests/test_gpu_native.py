@@ -9,8 +9,12 @@ from mats import AXT_PARAMS, CASES, case, within_bound
 
 pytestmark = pytest.mark.gpu
 
+# beyond the reference's parameter sets: tileH 2 (its own 2-wide kernel), 3 and 5 (tile
+# columns shorter than the kernel's lane width)
+EXTRA_AXT = [("COM", 2, 32, 256), ("COM", 3, 32, 256), ("COM", 5, 32, 256), ("UNC", 3, 32, 256)]
 FORMATS = [("CSR", {}), ("K1", {}), ("AXC", {"hbs": 32}), ("AXC", {"hbs": 16})] + [
-    ("AXT", {"mode": m, "tileH": th, "tileHW": thw, "bs": bs}) for (m, th, thw, bs) in AXT_PARAMS]
+    ("AXT", {"mode": m, "tileH": th, "tileHW": thw, "bs": bs})
+    for (m, th, thw, bs) in AXT_PARAMS + EXTRA_AXT]
 
 
 def _ids(p):
@@ -278,10 +282,11 @@ def test_lane_positions_padded32(port, kind, expect, fmt):
 
 @pytest.mark.parametrize("fmt", [dict(fmt="CSR"), dict(fmt="CSR", vtype="f32"),
                                  dict(fmt="AXT", mode="COM", tileH=1, tileHW=32),
+                                 dict(fmt="AXT", mode="COM", tileH=2, tileHW=32),
                                  dict(fmt="AXT", mode="COM", tileH=4, tileHW=32),
                                  dict(fmt="AXT", mode="COM", tileH=6, tileHW=32),
                                  dict(fmt="AXT", mode="UNC", tileH=6, tileHW=32)],
-                         ids=["csr", "csr-f32", "com1", "com4", "com6", "unc6"])
+                         ids=["csr", "csr-f32", "com1", "com2", "com4", "com6", "unc6"])
 def test_rows_across_warp_ranges(port, fmt):
     """Rows much longer than a warp's range of windows (up to 70,000 elements, next to empty
     and one-element rows; the warp where a row starts sums it past its range end): the bound

@@ -183,7 +183,7 @@ def test_dropin_products_per_row_and_metrics(lib, port, ref, name):
     check(lib.test_gaxc(256, a, R.f64p(y_ref)), "gaxc")
     R.free_struct_arrays(a, ("ax", "brp", "mapx"))
 
-    for (mode, th, thw, bs) in AXT_PARAMS:
+    for (mode, th, thw, bs) in AXT_PARAMS + [("COM", 2, 32, 256)]:
         t = L.StrMatAXT()
         fd = lib.getFormatDataAXT(1, bs, thw, th, mode.encode(), h.s, R.f64p(x), C.byref(t))
         rt = ref.axt(row, col, val, x, thw, th, mode, bs=bs)
