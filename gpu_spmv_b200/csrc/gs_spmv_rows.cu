@@ -904,13 +904,18 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
     rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, PADDED, EMPTY, T32, EARLY, 1>(a);
 }
 
-// Two owned tiles per step.  Register caps: 48 for tileH = 4 (5 blocks of 256 per SM), 40
-// for tileH = 2 (6 blocks); uncapped the compiler takes 56-64 and the x gathers in flight
-// per SM fall.
+// Two owned tiles per step.  Register caps: 48 for tileH = 4 (40 warps per SM), 40 for
+// tileH = 2 (48 warps); uncapped the compiler takes 56-64 and the x gathers in flight per SM
+// fall.
 constexpr int kGroupTiles = 2;
+// Blocks of 2 warps (one warp range each): a block's slot frees as soon as its two ranges
+// end, where a block of 8 waits for the slowest of 8 (power-law th=4 303.1 -> 298.6 us, 4
+// warps 299.4; th=2 unchanged).  The same registers: 20 / 24 blocks per SM.
+constexpr int kGroupedWarps = 2;
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool PADDED,
           bool EMPTY>
-__global__ void __launch_bounds__(256, V == 2 ? 6 : 5) k_rows_grouped(const RowsArgs a)
+__global__ void __launch_bounds__(32 * kGroupedWarps, (V == 2 ? 48 : 40) / kGroupedWarps)
+    k_rows_grouped(const RowsArgs a)
 {
     rows_aligned<VT, IT, XT, PT, AT, YT, V, true, false, PADDED, EMPTY, true, true,
                  kGroupTiles>(a);
@@ -1252,7 +1257,9 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
     // th=4 276 against 301 us)
     if constexpr (TILED && !BAKED && (V == 2 || V == 4)) {
         if (t32 && a.grouped) {
-#define GS_G(P, E) k_rows_grouped<VT, IT, XT, PT, AT, YT, V, P, E><<<blocks, 256, 0, s>>>(a)
+            const uint32_t gblocks = (warps + kGroupedWarps - 1) / kGroupedWarps;
+#define GS_G(P, E)                                                                          \
+    k_rows_grouped<VT, IT, XT, PT, AT, YT, V, P, E><<<gblocks, 32 * kGroupedWarps, 0, s>>>(a)
             if (padded) {
                 if (empty) GS_G(true, true); else GS_G(true, false);
             } else {
