@@ -903,6 +903,18 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
 {
     rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, PADDED, EMPTY, T32, EARLY, 1>(a);
 }
+// The same kernel in blocks of 2 warps, for the 32-wide tiles where that measured faster:
+// tileH 16 (power-law 458.8 -> 365.2 us, 27-point stencil 385.7 -> 359.2; 80 registers, 12
+// blocks per SM) and tileH 8 with x baked in (drop-in gaxtuh th=8 218.2 -> 211.9); slower
+// or level elsewhere (run-time-x th=8 on the stencil 321.7 -> 326.6, th=4 275.8 -> 282.6,
+// baked th=4 193.6 -> 205.5).
+template <int V, bool BAKED> constexpr bool kAlignedSmallBlocks = V == 16 || (V == 8 && BAKED);
+template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY, bool T32 = false, bool EARLY = false>
+__global__ void __launch_bounds__(64, V == 16 ? 12 : 20) k_rows_aligned2(const RowsArgs a)
+{
+    rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, PADDED, EMPTY, T32, EARLY, 1>(a);
+}
 
 // Two owned tiles per step.  Register caps: 48 for tileH = 4 (40 warps per SM), 40 for
 // tileH = 2 (48 warps); uncapped the compiler takes 56-64 and the x gathers in flight per SM
@@ -1270,11 +1282,19 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
             return GS_OK;
         }
     }
+#define GS_T32_LAUNCH(P, E)                                                                 \
+    do {                                                                                    \
+        if constexpr (TILED && kAlignedSmallBlocks<V, BAKED>)                               \
+            k_rows_aligned2<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED,           \
+                            TILED && !BAKED><<<(warps + 1) / 2, 64, 0, s>>>(a);             \
+        else                                                                                \
+            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED,            \
+                           TILED && !BAKED><<<blocks, 256, 0, s>>>(a);                      \
+    } while (0)
 #define GS_L(P, E)                                                                          \
     do {                                                                                    \
         if (t32)                                                                            \
-            k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, TILED, TILED && !BAKED> \
-                <<<blocks, 256, 0, s>>>(a);                                                 \
+            GS_T32_LAUNCH(P, E);                                                            \
         else                                                                                \
             k_rows_aligned<VT, IT, XT, PT, AT, YT, V, TILED, BAKED, P, E, false>            \
                 <<<blocks, 256, 0, s>>>(a);                                                 \
@@ -1285,6 +1305,7 @@ gs_status launch_aligned(const RowsArgs &a, bool padded, cudaStream_t s)
         if (empty) GS_L(false, true); else GS_L(false, false);
     }
 #undef GS_L
+#undef GS_T32_LAUNCH
     GS_CHECK_LAUNCH();
     return GS_OK;
 }
