@@ -570,15 +570,15 @@ __device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int la
 // the layout has padding positions (real-bit map).  EMPTY: some rows are empty.
 template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
           bool BAKED, bool PADDED, bool EMPTY>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
+__device__ __forceinline__ void rows_generic(const RowsArgs &a)
 {
     const int lane = threadIdx.x & 31;
     YT *y = static_cast<YT *>(a.y);
     const uint32_t V = TILED ? a.th : (uint32_t)VM;
     const uint32_t FULLV = (V >= 32) ? 0xffffffffu : ((1u << V) - 1u);
     const uint32_t WS = 32u * V;
-    const uint32_t nwarps = gridDim.x * kWarpsPerBlock;
-    const uint32_t gw = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 
     if constexpr (EMPTY) {
         for (uint32_t i = gw * 32 + lane; i < a.n_empty; i += nwarps * 32)
@@ -610,6 +610,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
             finish_overhang<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, PADDED, EMPTY>(
                 a, y, lane, w1, V, FULLV, cnt, carry);
     }
+}
+
+template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
+{
+    rows_generic<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, PADDED, EMPTY>(a);
+}
+// The same kernel in blocks of 2 warps, for the FP64 layouts where that measured faster
+// (the same bits): direct layouts, i.e. CSR, AXC and COM tileH 1 (power-law CSR 324.3 ->
+// 323.0 us, 27-point stencil 321.3 -> 313.7; drop-in gaxtch1 205 -> 198.5, 307.5 -> 295.3)
+// and tiled tileH 2 (power-law COM th=2 402 -> 389.5, stencil 575 -> 551).  Tiled tileH
+// 4 / 8 / 16 stay in blocks of 8 warps, where 2-warp blocks were slower (power-law COM
+// th=4 357 -> 394, th=8 345 -> 367, th=16 623 -> 675).  The minimum block counts cap the
+// registers at 48 (4 positions per lane) and 56 (8 per lane, tileH 2) without spills on
+// the run-time-x forms.
+template <class VT, int VM, bool TILED>
+constexpr bool kGenericSmallBlocks = std::is_same<VT, double>::value && (!TILED || VM == 2);
+template <int VM, bool TILED> constexpr int kGenericMinBlocks2 = (!TILED && VM == 4) ? 21 : 18;
+template <class VT, class IT, class XT, class PT, class AT, class YT, int VM, bool TILED,
+          bool BAKED, bool PADDED, bool EMPTY>
+__global__ void __launch_bounds__(64, kGenericMinBlocks2<VM, TILED>) k_rows2(const RowsArgs a)
+{
+    rows_generic<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, PADDED, EMPTY>(a);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1235,6 +1259,18 @@ gs_status launch_k(const RowsArgs &a, bool padded, cudaStream_t s)
     // the division gone the 64 registers it needs cost more than it hides (power-law COM
     // th=4 380 -> 364 us without it, th=2 500 -> 476; drop-in gaxtch th=4 326 -> 295;
     // 27-point stencil th=4 478 -> 454), so every window loads just before its use.
+    if constexpr (kGenericSmallBlocks<VT, VM, TILED>) {
+#define GS_D(P, E)                                                                          \
+    k_rows2<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E><<<(warps + 1) / 2, 64, 0, s>>>(a)
+        if (padded) {
+            if (empty) GS_D(true, true); else GS_D(true, false);
+        } else {
+            if (empty) GS_D(false, true); else GS_D(false, false);
+        }
+#undef GS_D
+        GS_CHECK_LAUNCH();
+        return GS_OK;
+    }
 #define GS_L(P, E)                                                                          \
     k_rows<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, P, E><<<blocks, kWarpsPerBlock * 32, 0, s>>>(a)
     if (padded) {
