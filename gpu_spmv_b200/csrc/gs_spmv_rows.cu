@@ -57,12 +57,30 @@ constexpr int kTmaWarps = 4;   // warps per block of the TMA kernel
 constexpr int kTmaStages = 4;  // tiles in flight per warp
 constexpr unsigned kFull = 0xffffffffu;
 
+
 // exact product / sum, never contracted into FMA (the reference's CPU loop multiplies and
 // adds separately)
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// Segmented inclusive warp scan of S: sstart is the lane of the row start at or before
+// this lane (-1: the row began before the window).  Level d adds lane - d into a lane only
+// where lane - d >= sstart, i.e. where the lane's run (lane - sstart) is at least d.  SPAN:
+// levels above the warp's longest run, which add nothing anywhere, are skipped after one
+// max-reduction of the runs; the sums and their order are those of the five-level scan.
+template <bool SPAN, class AT> __device__ __forceinline__ void seg_scan(AT &S, int lane, int sstart)
+{
+    uint32_t span = 32u;
+    if constexpr (SPAN) span = __reduce_max_sync(kFull, (uint32_t)(lane - sstart));
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        if (SPAN && (uint32_t)d > span) break;
+        AT t = __shfl_up_sync(kFull, S, d);
+        if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
+    }
+}
 
 // ---- streaming loads of 8 consecutive elements from an 8-element-aligned index
 template <class T> struct Load8;
@@ -246,9 +264,16 @@ __device__ __forceinline__ WinCtl window_ctl(int lane, uint32_t W, uint32_t V, u
 // tiled ones of 4 (COM th=4 on the power-law 358 -> 380) and 16 (COM th=16 624 -> 872).
 template <int VM, bool TILED>
 constexpr bool kBallotRanks = TILED ? (VM == 8 || VM == 2) : VM == 4;
+// Span-limited scans (seg_scan) where they measured faster, FP64 with x gathered at run
+// time: direct layouts (power-law CSR 323.0 -> 320.9 us, 27-point stencil 313.8 -> 309.4)
+// and tiled tileH 8 (COM th=8 345.2 -> 343.3, 394.0 -> 389.8).  Tiled tileH 2 and 4 keep
+// the full scan (COM th=2 390 -> 398, th=4 357.5 -> 358.4 with it), and so do the baked
+// layouts (drop-in gaxtch1 199 -> 200.6).
+template <class VT, int VM, bool TILED, bool BAKED>
+constexpr bool kScanSpan = std::is_same<VT, double>::value && !BAKED && (!TILED || VM == 8);
 
 // Row ranks, sequential lane sums, segmented warp scan, y writes and the window carry.
-template <class AT, class YT, int VM, bool EMPTY, class PT, bool BR>
+template <class AT, class YT, int VM, bool EMPTY, class PT, bool BR, bool SPAN = false>
 __device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane, uint32_t W,
                                               uint32_t V, uint32_t sraw, uint32_t vmask,
                                               uint32_t rb, const PT (&prod)[VM], uint32_t &cnt,
@@ -323,11 +348,7 @@ __device__ __forceinline__ void window_reduce(const RowsArgs &a, YT *y, int lane
     const unsigned le = rmask & (kFull >> (31 - lane));
     const int sstart = le ? 31 - __clz(le) : -1;
     AT S = acc;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        AT t = __shfl_up_sync(kFull, S, d);
-        if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
-    }
+    seg_scan<SPAN>(S, lane, sstart);
     if (sstart < 0) S = add_rn(S, carry);
     AT E = __shfl_up_sync(kFull, S, 1);
     if (lane == 0) E = carry;
@@ -557,7 +578,8 @@ __device__ __forceinline__ void finish_overhang(const RowsArgs &a, YT *y, int la
         const uint32_t rb = PADDED ? (get_bits(a.rbits, qb, V) & ctl.vmask) : ctl.vmask;
         PT prod[VM];
         products_ldg<VT, IT, XT, PT, VM, TILED, BAKED>(a, w, qb, V, rb, prod);
-        window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>>(
+        window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>,
+                      kScanSpan<VT, VM, TILED, BAKED>>(
             a, y, lane, W, V, sraw, ctl.vmask, rb, prod, cnt, carry);
         if (ctl.slanes != 0u) break;  // the last row ended in this window
     }
@@ -602,7 +624,8 @@ __device__ __forceinline__ void rows_generic(const RowsArgs &a)
             const uint32_t rb = cur.rraw & ctl.vmask;
             PT prod[VM];
             win_products<VT, IT, XT, PT, VM, BAKED>(a, w, V, cur, rb, prod);
-            window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>>(
+            window_reduce<AT, YT, VM, EMPTY, PT, kBallotRanks<VM, TILED>,
+                          kScanSpan<VT, VM, TILED, BAKED>>(
                 a, y, lane, W, V, cur.sraw, ctl.vmask, rb, prod, cnt, carry);
             seen = true;
         }
@@ -898,11 +921,13 @@ __device__ __forceinline__ void rows_aligned(const RowsArgs &a)
             const unsigned le = sm & mine;
             const int sstart = le ? 31 - __clz(le) : -1;
             AT S = acc;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                AT t = __shfl_up_sync(kFull, S, d);
-                if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
-            }
+            // span-limited for FP64 with x gathered at run time, one tile per step
+            // (power-law UNC th=8 335.0 -> 331.7 us, th=16 365.5 -> 363.9, AXC 433.6 ->
+            // 429.5; 27-point stencil UNC th=4 276.0 -> 270.3, th=2 363.0 -> 359.2, AXC
+            // 325.2 -> 321.2); the two-tile kernel (power-law UNC th=4 299.0 -> 299.7 with
+            // it, th=2 325.6 -> 326.6) and the baked layouts (drop-in gaxtuh th=4 191 ->
+            // 192) keep the full scan
+            seg_scan<std::is_same<VT, double>::value && !BAKED && NT == 1>(S, lane, sstart);
             if (sstart < 0) S = add_rn(S, carry);
             bool nxt;
             if (lane < 31) nxt = (smask >> (lane + 1)) & 1u;
@@ -992,11 +1017,7 @@ __device__ __forceinline__ bool stripe_chunk(const RowsArgs &a, YT *y, int lane,
     const unsigned le = sw & mine;
     const int sstart = le ? 31 - __clz(le) : -1;
     AT S = valid ? (AT)prod : (AT)0;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        AT t = __shfl_up_sync(kFull, S, d);
-        if (lane >= d && lane - d >= sstart) S = add_rn(S, t);
-    }
+    seg_scan<false>(S, lane, sstart);
     if (sstart < 0) S = add_rn(S, carry);
     // does the row in progress at this lane end here?
     bool nxt;
