@@ -975,7 +975,10 @@ constexpr int kGroupTiles = 2;
 constexpr int kGroupedWarps = 2;
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool PADDED,
           bool EMPTY>
-__global__ void __launch_bounds__(32 * kGroupedWarps, (V == 2 ? 48 : 40) / kGroupedWarps)
+#ifndef GS_GRP4
+#define GS_GRP4 40
+#endif
+__global__ void __launch_bounds__(32 * kGroupedWarps, (V == 2 ? 48 : GS_GRP4) / kGroupedWarps)
     k_rows_grouped(const RowsArgs a)
 {
     rows_aligned<VT, IT, XT, PT, AT, YT, V, true, false, PADDED, EMPTY, true, true,
