@@ -967,7 +967,7 @@ __global__ void __launch_bounds__(64, V == 16 ? 12 : 20) k_rows_aligned2(const R
 
 // Two owned tiles per step.  Register caps: 48 for tileH = 4 (40 warps per SM), 40 for
 // tileH = 2 (48 warps); uncapped the compiler takes 56-64 and the x gathers in flight per SM
-// fall.
+// fall.  TileH 4 at 40 registers (48 warps) spills 32 bytes: power-law 299.9 -> 323.6 us.
 constexpr int kGroupTiles = 2;
 // Blocks of 2 warps (one warp range each): a block's slot frees as soon as its two ranges
 // end, where a block of 8 waits for the slowest of 8 (power-law th=4 303.1 -> 298.6 us, 4
@@ -975,10 +975,7 @@ constexpr int kGroupTiles = 2;
 constexpr int kGroupedWarps = 2;
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool PADDED,
           bool EMPTY>
-#ifndef GS_GRP4
-#define GS_GRP4 40
-#endif
-__global__ void __launch_bounds__(32 * kGroupedWarps, (V == 2 ? 48 : GS_GRP4) / kGroupedWarps)
+__global__ void __launch_bounds__(32 * kGroupedWarps, (V == 2 ? 48 : 40) / kGroupedWarps)
     k_rows_grouped(const RowsArgs a)
 {
     rows_aligned<VT, IT, XT, PT, AT, YT, V, true, false, PADDED, EMPTY, true, true,
