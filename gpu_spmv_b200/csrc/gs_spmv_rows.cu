@@ -646,9 +646,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 // 323.0 us, 27-point stencil 321.3 -> 313.7; drop-in gaxtch1 205 -> 198.5, 307.5 -> 295.3)
 // and tiled tileH 2 (power-law COM th=2 402 -> 389.5, stencil 575 -> 551).  Tiled tileH
 // 4 / 8 / 16 stay in blocks of 8 warps, where 2-warp blocks were slower (power-law COM
-// th=4 357 -> 394, th=8 345 -> 367, th=16 623 -> 675).  The minimum block counts cap the
-// registers at 48 (4 positions per lane) and 56 (8 per lane, tileH 2) without spills on
-// the run-time-x forms.
+// th=4 357 -> 394 at 56 registers and 357 -> 366 at the same 48, th=8 345 -> 367, th=16
+// 623 -> 675).  The minimum block counts cap the registers at 48 (4 positions per lane) and
+// 56 (8 per lane, tileH 2) without spills on the run-time-x forms.
 template <class VT, int VM, bool TILED>
 constexpr bool kGenericSmallBlocks = std::is_same<VT, double>::value && (!TILED || VM == 2);
 template <int VM, bool TILED> constexpr int kGenericMinBlocks2 = (!TILED && VM == 4) ? 21 : 18;
