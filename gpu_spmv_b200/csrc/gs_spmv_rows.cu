@@ -57,7 +57,6 @@ constexpr int kTmaWarps = 4;   // warps per block of the TMA kernel
 constexpr int kTmaStages = 4;  // tiles in flight per warp
 constexpr unsigned kFull = 0xffffffffu;
 
-
 // exact product / sum, never contracted into FMA (the reference's CPU loop multiplies and
 // adds separately)
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -642,7 +641,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
     rows_generic<VT, IT, XT, PT, AT, YT, VM, TILED, BAKED, PADDED, EMPTY>(a);
 }
 // The same kernel in blocks of 2 warps, for the FP64 layouts where that measured faster
-// (the same bits): direct layouts, i.e. CSR, AXC and COM tileH 1 (power-law CSR 324.3 ->
+// (the same bits): direct layouts, i.e. CSR and COM tileH 1 (power-law CSR 324.3 ->
 // 323.0 us, 27-point stencil 321.3 -> 313.7; drop-in gaxtch1 205 -> 198.5, 307.5 -> 295.3)
 // and tiled tileH 2 (power-law COM th=2 402 -> 389.5, stencil 575 -> 551).  Tiled tileH
 // 4 / 8 / 16 stay in blocks of 8 warps, where 2-warp blocks were slower (power-law COM
