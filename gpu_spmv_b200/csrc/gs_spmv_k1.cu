@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(256, std::is_same<VT, double>::value
         // the last 1-7 slots of this lane.  FP32 / BF16 values with 32-bit columns: loads
         // first, as one batch (5 % faster on the 27-point stencil); FP64 the same when the
         // whole chunk is shorter than 8 steps (its rows are all tail), else the plain loop,
-        // as for 16-bit steps, which measured faster for them
+        // as for 16-bit steps, which measured faster for them (27-point stencil FP32 values
+        // with 16-bit steps: 132.0 us plain, 133.7 / 135.7 batched 4 / 8 at a time)
         constexpr bool kF64 = std::is_same<VT, double>::value;
         const bool batch_tail = !kDelta && (!kF64 || nmc < 8u);
         for (; !batch_tail && j < j1; j++) {
