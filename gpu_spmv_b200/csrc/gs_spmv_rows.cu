@@ -266,8 +266,8 @@ constexpr bool kBallotRanks = TILED ? (VM == 8 || VM == 2) : VM == 4;
 // Span-limited scans (seg_scan) where they measured faster, FP64 with x gathered at run
 // time: direct layouts (power-law CSR 323.0 -> 320.9 us, 27-point stencil 313.8 -> 309.4)
 // and tiled tileH 8 (COM th=8 345.2 -> 343.3, 394.0 -> 389.8).  Tiled tileH 2 and 4 keep
-// the full scan (COM th=2 390 -> 398, th=4 357.5 -> 358.4 with it), and so do the baked
-// layouts (drop-in gaxtch1 199 -> 200.6).
+// the full scan (COM th=2 390 -> 398, th=4 357.5 -> 358.4 with it), and so do tileH 16
+// (COM th=16 623.5 -> 626.0) and the baked layouts (drop-in gaxtch1 199 -> 200.6).
 template <class VT, int VM, bool TILED, bool BAKED>
 constexpr bool kScanSpan = std::is_same<VT, double>::value && !BAKED && (!TILED || VM == 8);
 
