@@ -648,7 +648,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_rows(const RowsArgs a)
 // th=4 357 -> 394 at 56 registers and 357 -> 366 at the same 48, th=8 345 -> 367, th=16
 // 623 -> 675).  The minimum block counts cap the registers at 48 (4 positions per lane) and
 // 56 (8 per lane, tileH 2) without spills on the run-time-x forms (32 registers for 4 per
-// lane would spill 16-36 bytes).
+// lane would spill 16-36 bytes).  FP32 / BF16 values keep blocks of 8 and the five-level
+// scan: with both, CSR FP32 on the 27-point stencil 213.5 -> 237.0 us, on the power-law
+// 310 -> 322; BF16 on the power-law 299 -> 342.
 template <class VT, int VM, bool TILED>
 constexpr bool kGenericSmallBlocks = std::is_same<VT, double>::value && (!TILED || VM == 2);
 template <int VM, bool TILED> constexpr int kGenericMinBlocks2 = (!TILED && VM == 4) ? 21 : 18;
