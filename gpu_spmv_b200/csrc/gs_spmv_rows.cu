@@ -959,7 +959,8 @@ __global__ void __launch_bounds__(256) k_rows_aligned(const RowsArgs a)
 // blocks per SM) and tileH 8 with x baked in (drop-in gaxtuh th=8 218.2 -> 211.9); slower
 // or level elsewhere (run-time-x th=8 on the stencil 321.7 -> 326.6, 320.4 -> 324.5 with the
 // span-limited scan, on the power-law 331.6 either way; th=4 275.8 -> 282.6, baked th=4
-// 193.6 -> 205.5).
+// 193.6 -> 205.5; the direct AXC / UNC th=1 hw32 layouts at the same 32 / 40 registers:
+// power-law 430 -> 433, stencil 321.8 -> 322.7).
 template <int V, bool BAKED> constexpr bool kAlignedSmallBlocks = V == 16 || (V == 8 && BAKED);
 template <class VT, class IT, class XT, class PT, class AT, class YT, int V, bool TILED,
           bool BAKED, bool PADDED, bool EMPTY, bool T32 = false, bool EARLY = false>
